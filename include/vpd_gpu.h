@@ -1,0 +1,243 @@
+/*
+ * vpd_gpu.h -- C ABI of the B200 correspondence-peridynamics increment (libvpd_gpu.so).
+ *
+ * Plain C types only: pointers, sizes and status codes. Every entry point returns an
+ * int status (VPD_OK == 0); vpd_last_error() gives a message for the calling thread's
+ * last failure. A handle owns device state and one CUDA stream; it is not thread-safe.
+ *
+ * Reference interfaces each entry point replaces (paths inside 1998yu/vumat-pd):
+ *   vpd_create               makeParticlePatch (src/host/Geometry.cpp:10-34)
+ *                            + buildNeighborList (src/pd/PdCorrespondenceSkeleton.cpp:95-129)
+ *                            + PdCorrespondenceSkeleton::initialize (:149-170)
+ *                            + RegionalConstraintSystem ctor (src/host/BoundaryConditions.cpp:54-68)
+ *                            + VumatPdCorrespondenceMaterial::initialize
+ *                              (src/material/VumatPdCorrespondenceMaterial.cpp:48-70)
+ *                            + runMaterial set-up (src/host/BoundaryValueCaseRunner.cpp:142-190)
+ *   vpd_step                 the step loop of runMaterial (BoundaryValueCaseRunner.cpp:207-306):
+ *                            predictDisplacement, constraints.apply, computeDeformationGradients,
+ *                            bridge.update (kinematics + VUMAT), PdSimpleDamage::update,
+ *                            computeForceDensity, correctVelocity, constraints.apply, diagnostics
+ *   vpd_download             the per-node fields written by writeSnapshot
+ *                            (BoundaryValueCaseRunner.cpp:115-137) and the MaterialState /
+ *                            ExplicitDynamicState members (include/PdTypes.hpp:25-47,
+ *                            include/ExplicitTimeIntegrator.hpp:10-13)
+ *   vpd_neighbors            ParticleBlock::neighbors (include/PdTypes.hpp:18) as CSR
+ *   vpd_build_neighbor_list  buildNeighborList (PdCorrespondenceSkeleton.cpp:95-129)
+ *   vpd_shape_tensor_inverse PdCorrespondenceSkeleton::initialize (:149-170)
+ *   vpd_deformation_gradients PdCorrespondenceSkeleton::computeDeformationGradients (:172-197)
+ *   vpd_force_density        PdCorrespondenceSkeleton::computeForceDensity (:199-230)
+ *   vpd_corotational_update  updateCorotationalKinematics, greenLagrangeStrain
+ *                            (src/pd/CorotationalKinematics.cpp:61-149)
+ *   vpd_material_update      VumatPdCorrespondenceMaterial::update (:72-176) with the
+ *                            Johnson-Cook VUMAT (materials/examples/JohnsonCook.f90:12-172)
+ *   vpd_damage_update        PdSimpleDamage::update, critical_stretch (src/damage/PdSimpleDamage.cpp:51-96)
+ *   vumat_adapter_call       the plugin entry the reference dlopens
+ *                            (materials/bridge/vumat_c_wrapper_jinfo.f90:1-17,
+ *                             include/VumatMaterialAdapter.hpp:35-39), Johnson-Cook on the GPU
+ *
+ * Module-level entry points (vpd_build_neighbor_list ... vpd_damage_update) take DEVICE
+ * pointers owned by the caller and a cudaStream_t passed as void*; they run on that stream
+ * and return after the work is queued unless stated otherwise. Tensors are row-major 3x3
+ * (9 doubles per point, point-major), vectors 3 doubles per point, as the reference's
+ * Tensor3/Vec3 (include/PdTypes.hpp:9-10).
+ */
+#ifndef VPD_GPU_H
+#define VPD_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VPD_ABI_VERSION 1
+
+/* Status codes. */
+enum {
+  VPD_OK = 0,
+  VPD_ERR_INVALID = 1,     /* bad argument or configuration (reference: std::runtime_error) */
+  VPD_ERR_CUDA = 2,        /* CUDA runtime error */
+  VPD_ERR_SINGULAR = 3,    /* |det| < 1e-14 in K, F or a kinematics inverse */
+  VPD_ERR_NONFINITE = 4,   /* non-finite coordinate or state */
+  VPD_ERR_CAPACITY = 5,    /* neighbour row or cell grid beyond the supported size */
+  VPD_ERR_UNSUPPORTED = 6  /* configuration the device path does not implement */
+};
+
+enum { VPD_BC_SMOOTH_DISPLACEMENT = 0, VPD_BC_VELOCITY_RAMP = 1 };
+enum { VPD_DAMAGE_NONE = 0, VPD_DAMAGE_CRITICAL_STRETCH = 1 };
+enum { VPD_PRECISION_FP64 = 0, VPD_PRECISION_MIXED = 1 };
+enum { VPD_MATERIAL_VUMAT = 0, VPD_MATERIAL_SURROGATE = 1 };
+
+/*
+ * One regional boundary-value case (the fields of DemoCaseConfig that the PD increment uses,
+ * include/DemoConfig.hpp:71-167), in the reference's mm-ms-N-MPa units.
+ */
+typedef struct vpd_case {
+  /* geometry: a nx*ny*nz lattice, index (i*ny + j)*nz + k, x from 0, y and z centred */
+  int32_t nx, ny, nz;
+  double spacing;          /* h, mm */
+  double horizon;          /* delta, mm */
+  double jitter;           /* uniform position jitter amplitude as a fraction of h (0: none) */
+  uint64_t jitter_seed;
+  /* time integration */
+  double dt;               /* ms */
+  double density;          /* dynamics.density, N ms^2 / mm^4 */
+  /* boundary conditions */
+  int32_t bc_mode;         /* VPD_BC_* */
+  int32_t load_axis;       /* 0: x, left support / right load; 1: y, bottom / top */
+  int32_t region_layers;   /* constrained nodal planes per band */
+  int32_t plane_strain;    /* 1: all z displacement constrained */
+  double amplitude;        /* smooth displacement: end displacement, mm */
+  double rise_time;        /* smooth displacement: half-cosine rise, ms */
+  double grip_velocity;    /* velocity ramp: relative speed of the two bands, mm/ms */
+  double ramp_time;        /* velocity ramp: linear ramp duration, ms */
+  double observation_min;  /* observation window along the load axis, mm; NaN: band edges */
+  double observation_max;
+  /* material: Johnson-Cook props E, nu, A, B, C, n, m, rate0, Tref, Tmelt, rho, beta, Cp,
+     workToHeat (materials/examples/JohnsonCook.f90:9) */
+  double props[14];
+  int32_t nstatev;         /* >= 6 */
+  double reference_temperature;
+  /* damage (PdSimpleDamage, critical_stretch) */
+  int32_t damage_mode;     /* VPD_DAMAGE_* */
+  double damage_initiation;
+  double damage_failure;   /* > 0 enables the compression threshold */
+  /* numerics */
+  int32_t precision;       /* VPD_PRECISION_* */
+  int32_t material_mode;   /* VPD_MATERIAL_* */
+} vpd_case;
+
+/* Per-step diagnostic row: the numeric columns of timeseries.csv in the reference's order
+   (BoundaryValueCaseRunner.cpp:347-351, values :309-315). */
+enum {
+  VPD_DIAG_STEP = 0,
+  VPD_DIAG_TIME,
+  VPD_DIAG_LOAD_DISPLACEMENT,
+  VPD_DIAG_LOAD_VELOCITY,
+  VPD_DIAG_REACTION,
+  VPD_DIAG_ENGINEERING_STRAIN,
+  VPD_DIAG_LATERAL_STRAIN,
+  VPD_DIAG_NOMINAL_STRESS,
+  VPD_DIAG_AVERAGE_AXIAL_STRAIN,
+  VPD_DIAG_AVERAGE_AXIAL_STRESS,
+  VPD_DIAG_MAX_EQPS,
+  VPD_DIAG_MAX_INTERNAL_INDICATOR,
+  VPD_DIAG_KINETIC_ENERGY,
+  VPD_DIAG_INTERNAL_ENERGY,
+  VPD_DIAG_EXTERNAL_WORK,
+  VPD_DIAG_ENERGY_ERROR,
+  VPD_DIAG_NET_INTERNAL_FORCE,
+  VPD_DIAG_FINITE,
+  VPD_DIAG_COLS
+};
+
+/* Fields for vpd_download; widths per point in brackets. */
+enum {
+  VPD_FIELD_POSITION = 0,     /* [3] reference position */
+  VPD_FIELD_VOLUME,           /* [1] */
+  VPD_FIELD_DISPLACEMENT,     /* [3] */
+  VPD_FIELD_VELOCITY,         /* [3] */
+  VPD_FIELD_ACCELERATION,     /* [3] */
+  VPD_FIELD_DEFGRAD,          /* [9] F at the end of the last increment */
+  VPD_FIELD_STRESS_COROTATIONAL, /* [9] VUMAT stress, corotational frame */
+  VPD_FIELD_STRESS_SPATIAL,   /* [9] R sigma R^T, as used by the force state */
+  VPD_FIELD_STRAIN,           /* [9] Green-Lagrange strain */
+  VPD_FIELD_ROTATION,         /* [9] */
+  VPD_FIELD_LEFT_STRETCH,     /* [9] */
+  VPD_FIELD_STATE,            /* [nstatev] VUMAT state variables */
+  VPD_FIELD_TEMPERATURE,      /* [1] */
+  VPD_FIELD_ENERGY_INTERNAL,  /* [1] */
+  VPD_FIELD_ENERGY_INELASTIC, /* [1] */
+  VPD_FIELD_DAMAGE_INDEX,     /* [1] volume-weighted broken-bond fraction */
+  VPD_FIELD_FORCE_DENSITY,    /* [3] force density of the last increment */
+  VPD_FIELD_SHAPE_INVERSE,    /* [9] K^-1 */
+  VPD_FIELD_COUNT
+};
+
+typedef struct vpd_handle vpd_handle;
+
+int vpd_abi_version(void);
+const char *vpd_last_error(void);
+/* Width (doubles per point) of a field for a handle's case. */
+int vpd_field_width(const vpd_handle *h, int field);
+
+/* Builds the lattice, neighbour lists and K^-1 on the device and initialises the state.
+   positions/volumes may be NULL (lattice from the case) or host arrays of n_points*3 and
+   n_points doubles that replace the lattice's coordinates (the lattice still defines the
+   boundary bands and observation window, which need nx*ny*nz == n_points). */
+int vpd_create(const vpd_case *c, const double *positions, const double *volumes,
+               vpd_handle **out);
+int vpd_destroy(vpd_handle *h);
+int64_t vpd_num_points(const vpd_handle *h);
+int64_t vpd_num_bonds(const vpd_handle *h);
+/* Advances nsteps increments. diag_out (host, may be NULL) receives nsteps rows of
+   VPD_DIAG_COLS doubles. Returns after the increments completed on the device. */
+int vpd_step(vpd_handle *h, int32_t nsteps, double *diag_out);
+/* Copies a field of every point into host memory (n_points * width doubles). */
+int vpd_download(vpd_handle *h, int32_t field, double *host_out);
+/* Canonical neighbour lists: row_ptr[n_points+1] and col[n_bonds], host memory, each row
+   ascending as ParticleBlock::neighbors. */
+int vpd_neighbors(vpd_handle *h, int64_t *row_ptr, int32_t *col);
+/* The handle's CUDA stream (cudaStream_t) and device-side time of its last vpd_step. */
+void *vpd_stream(vpd_handle *h);
+int vpd_last_step_ms(const vpd_handle *h, double *ms);
+
+/* ---- module-level entry points (device pointers, caller-owned) ---- */
+
+/* Sorted neighbour lists of n points (positions n*3 doubles). First call with col == NULL:
+   fills row_ptr[n+1] and *total. Second call with col of *total ints fills the rows. Both
+   calls synchronise the stream. Scratch memory is allocated and freed internally. */
+int vpd_build_neighbor_list(const double *positions, int64_t n, double horizon,
+                            int64_t *row_ptr, int32_t *col, int64_t *total, void *stream);
+int vpd_shape_tensor_inverse(const double *positions, const double *volumes, int64_t n,
+                             const int64_t *row_ptr, const int32_t *col, double *kinv,
+                             void *stream);
+int vpd_deformation_gradients(const double *positions, const double *displacement,
+                              const double *volumes, int64_t n, const int64_t *row_ptr,
+                              const int32_t *col, const double *kinv, double *defgrad,
+                              void *stream);
+/* bond_damage: one double per CSR entry (PdDamageState::bondDamageN). */
+int vpd_force_density(const double *positions, const double *volumes, int64_t n,
+                      const int64_t *row_ptr, const int32_t *col, const double *kinv,
+                      const double *defgrad, const double *cauchy_stress,
+                      const double *bond_damage, double *force, void *stream);
+/* Per point: F_n, F_n+1, V_n, R_n -> D-bar (unrotated rate of deformation), relative spin
+   increment, R_n+1, V_n+1, Green-Lagrange E(F_n+1); all [9] per point. */
+int vpd_corotational_update(int64_t n, const double *defgrad_old, const double *defgrad_new,
+                            const double *stretch_old, const double *rotation_old, double dt,
+                            double *rate_of_deformation, double *relative_spin,
+                            double *rotation_new, double *stretch_new, double *strain_new,
+                            void *stream);
+/* The material bridge on device state (updated in place): defgrad_old, stretch, rotation,
+   strain, stress_corotational [9]; state [nstatev]; temperature, energies [1].
+   stress_spatial [9] receives R sigma R^T. props: 14 Johnson-Cook properties (host). */
+int vpd_material_update(int64_t n, const double *props, int32_t nstatev, double dt,
+                        const double *defgrad_new, double *defgrad_old, double *stretch,
+                        double *rotation, double *strain, double *stress_corotational,
+                        double *state, double *temperature, double *energy_internal,
+                        double *energy_inelastic, double *stress_spatial, void *stream);
+/* Critical-stretch bond breaking: bond_damage (per CSR entry, 0/1) updated in place,
+   damage_index [n] written. */
+int vpd_damage_update(const double *positions, const double *displacement,
+                      const double *volumes, int64_t n, const int64_t *row_ptr,
+                      const int32_t *col, double initiation, double failure,
+                      double *bond_damage, double *damage_index, void *stream);
+
+/* Plugin ABI: the Johnson-Cook VUMAT evaluated on the GPU for one block of host arrays
+   in the reference's column-major [component][nblock] layout. Synchronous. A failure is
+   reported on stderr and ends the process, as the Fortran routine's `stop` does. */
+void vumat_adapter_call(int *nblock, int *ndir, int *nshr, int *nstatev, int *nfieldv,
+                        int *nprops, int *lanneal, double *stepTime, double *totalTime,
+                        double *dt, char *cmname, double *coordMp, double *charLength,
+                        double *props, double *density, double *strainInc, double *relSpinInc,
+                        double *tempOld, double *stretchOld, double *defgradOld, double *fieldOld,
+                        double *stressOld, double *stateOld, double *enerInternOld,
+                        double *enerInelasOld, double *tempNew, double *stretchNew,
+                        double *defgradNew, double *fieldNew, double *stressNew, double *stateNew,
+                        double *enerInternNew, double *enerInelasNew);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VPD_GPU_H */
