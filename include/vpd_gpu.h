@@ -181,6 +181,11 @@ int vpd_neighbors(vpd_handle *h, int64_t *row_ptr, int32_t *col);
 /* The handle's CUDA stream (cudaStream_t) and device-side time of its last vpd_step. */
 void *vpd_stream(vpd_handle *h);
 int vpd_last_step_ms(const vpd_handle *h, double *ms);
+/* Advances nsteps increments launching each kernel separately, with CUDA events between
+   them on the handle's stream; stage_ms[3] receives the mean device time of the
+   deformation, material and force kernels. Diagnostics rows are kept on the device only.
+   (No reference counterpart: per-stage timing of the step loop.) */
+int vpd_profile_increment(vpd_handle *h, int32_t nsteps, double *stage_ms);
 
 /* ---- module-level entry points (device pointers, caller-owned) ---- */
 

@@ -301,3 +301,39 @@ def ramp(case, t):
     out = np.zeros(6)
     oracle_lib().vo_ramp(ctypes.byref(case.to_c()), t, _dp(out))
     return out
+
+
+# ---------------------------------------------------------------- plugin ABI
+def vumat_block(lib, props, dt, strain_inc, stress_old, state_old, temp_old, e_int_old,
+                e_inel_old, nstatev=None, step_time=0.0, total_time=0.0):
+    """Calls `vumat_adapter_call` of a loaded plugin (the restated JC in libvpd_oracle.so, or
+    any library exporting the entry) on one block. Arrays are point-major [nblock, comps];
+    they are packed to the plugin's column-major [comp][nblock] layout and back."""
+    fn = lib.vumat_adapter_call
+    nb = strain_inc.shape[0]
+    nsv = nstatev or state_old.shape[1]
+    ci = ctypes.c_int
+    def col(a, comps):
+        return np.ascontiguousarray(np.asarray(a, dtype=np.float64).reshape(nb, comps).T)
+    inc, s_old, st_old = col(strain_inc, 6), col(stress_old, 6), col(state_old, nsv)
+    t_old = np.ascontiguousarray(temp_old, dtype=np.float64).reshape(nb)
+    ei_old = np.ascontiguousarray(e_int_old, dtype=np.float64).reshape(nb)
+    ep_old = np.ascontiguousarray(e_inel_old, dtype=np.float64).reshape(nb)
+    props = np.ascontiguousarray(props, dtype=np.float64)
+    zeros = lambda *shape: np.zeros(shape)
+    coord, char_len, dens = zeros(3, nb), np.ones(nb), np.full(nb, props[10])
+    spin, stretch_old, defgrad_old, field_old = zeros(3, nb), zeros(6, nb), zeros(9, nb), zeros(1, nb)
+    t_new, stretch_new, defgrad_new, field_new = zeros(nb), zeros(6, nb), zeros(9, nb), zeros(1, nb)
+    s_new, st_new, ei_new, ep_new = zeros(6, nb), zeros(nsv, nb), zeros(nb), zeros(nb)
+    cmname = ctypes.create_string_buffer(b" " * 80, 80)
+    args = [ctypes.byref(ci(nb)), ctypes.byref(ci(3)), ctypes.byref(ci(3)), ctypes.byref(ci(nsv)),
+            ctypes.byref(ci(1)), ctypes.byref(ci(len(props))), ctypes.byref(ci(0)),
+            ctypes.byref(ctypes.c_double(step_time)), ctypes.byref(ctypes.c_double(total_time)),
+            ctypes.byref(ctypes.c_double(dt)), cmname]
+    arrays = [coord, char_len, props, dens, inc, spin, t_old, stretch_old, defgrad_old, field_old,
+              s_old, st_old, ei_old, ep_old, t_new, stretch_new, defgrad_new, field_new, s_new,
+              st_new, ei_new, ep_new]
+    fn.restype = None
+    fn(*args, *[_dp(a) for a in arrays])
+    return {"stress": s_new.T.copy(), "state": st_new.T.copy(), "temperature": t_new,
+            "energy_internal": ei_new, "energy_inelastic": ep_new}

@@ -1,0 +1,45 @@
+import os
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+sys.path.insert(0, os.path.join(ROOT, "vumat-pd_b200"))
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200) and libvpd_gpu.so")
+
+
+def golden(name):
+    return os.path.join(GOLDEN, name)
+
+
+def nrmse(a, ref):
+    """RMS difference over peak |reference| (analyse_and_plot.py:66-74)."""
+    a, ref = np.asarray(a, float), np.asarray(ref, float)
+    peak = np.max(np.abs(ref))
+    return float(np.sqrt(np.mean((a - ref) ** 2)) / (peak if peak > 0 else 1.0))
+
+
+def max_rel(a, ref):
+    a, ref = np.asarray(a, float), np.asarray(ref, float)
+    scale = np.max(np.abs(ref))
+    return float(np.max(np.abs(a - ref)) / (scale if scale > 0 else 1.0))
+
+
+def load_golden_timeseries():
+    import csv
+    import gzip
+    with gzip.open(golden("pd_coarse_timeseries.csv.gz"), "rt") as f:
+        rows = list(csv.reader(f))
+    return rows[0][1:], np.array([[float(x) for x in r[1:]] for r in rows[1:]])
+
+
+@pytest.fixture(scope="session")
+def oracle():
+    import oracle as O
+    return O

@@ -1,0 +1,99 @@
+"""Regenerates the golden fixtures in this directory from the reference checkout.
+
+Run here (where the reference sources are mounted) after `make -C oracle`:
+
+    python tests/golden/make_golden.py /root/reference
+
+Fixtures (read by the tests; nothing at test time reads the reference checkout):
+  pd_coarse_timeseries.csv.gz  the reference's archived JC run
+                               benchmarks/tensile3d/raw/pd_coarse/timeseries.csv.gz (copied)
+  pd_coarse_snapshot.npz       the final-step nodal fields of that run
+                               (raw/pd_coarse/field_snapshots.csv.gz, step 4800)
+  ref_neighbors_jittered.npz   buildNeighborList of the reference library on a jittered
+                               17x9x5 lattice (delta = 3.015 h)
+  ref_tensile_bar_1.npz        the reference library (via oracle/_ref/libvpd_refharness.so,
+                               restated JC plugin) on the 40x10x10 velocity-ramp bar with
+                               +-0.05 h jitter and critical-stretch damage: 300 timeseries rows
+                               and the final displacement, stress and state
+  ref_jc_thermal.npz           one plastic step of the restated JC plugin (pinned bit for bit
+                               to the archived run above) with the inputs of the reference's
+                               tests/jc_thermal_units_test.cpp, for workToHeat 1 and 1e6
+"""
+import csv
+import gzip
+import os
+import shutil
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+sys.path.insert(0, os.path.join(ROOT, "vumat-pd_b200"))
+
+
+def main(reference):
+    import oracle as O
+    from vpd.case import Case, REFERENCE_JC_PROPS, tensile_bar
+
+    raw = os.path.join(reference, "benchmarks", "tensile3d", "raw", "pd_coarse")
+    shutil.copyfile(os.path.join(raw, "timeseries.csv.gz"),
+                    os.path.join(HERE, "pd_coarse_timeseries.csv.gz"))
+    with gzip.open(os.path.join(raw, "field_snapshots.csv.gz"), "rt") as f:
+        rows = list(csv.reader(f))
+    header, body = rows[0], rows[1:]
+    cols = {name: i for i, name in enumerate(header)}
+    last = [r for r in body if int(r[cols["step"]]) == 4800]
+    last.sort(key=lambda r: int(r[cols["particle"]]))
+
+    def column(name):
+        return np.array([float(r[cols[name]]) for r in last])
+
+    np.savez_compressed(
+        os.path.join(HERE, "pd_coarse_snapshot.npz"),
+        displacement=np.stack([column("ux_mm"), column("uy_mm"), column("uz_mm")], 1),
+        velocity=np.stack([column("vx_mm_per_ms"), column("vy_mm_per_ms"), column("vz_mm_per_ms")], 1),
+        axial_strain=column("axial_strain"), axial_stress=column("axial_stress_MPa"),
+        eqps=column("eqps"))
+
+    # neighbour lists of the reference library on a jittered lattice
+    small = Case(name="jittered", nx=17, ny=9, nz=5, spacing=1.25, horizon=3.015 * 1.25,
+                 dt=1e-5, steps=1, density=0.0078, props=REFERENCE_JC_PROPS, jitter=0.05,
+                 jitter_seed=11, grip_velocity=1.0, ramp_time=1e-3)
+    sim = O.RefSim(small)
+    pos = sim.get("position")
+    row_ptr, col = sim.neighbors()
+    np.savez_compressed(os.path.join(HERE, "ref_neighbors_jittered.npz"), positions=pos,
+                        horizon=small.horizon, row_ptr=row_ptr, col=col)
+    sim.close()
+
+    # the reference library on the 40x10x10 bar with jitter and damage
+    bar = tensile_bar(1, jitter=0.05, jitter_seed=7, damage_mode=1, damage_initiation=0.004)
+    sim = O.RefSim(bar)
+    diag = sim.step(300)
+    np.savez_compressed(os.path.join(HERE, "ref_tensile_bar_1.npz"), diag=diag,
+                        displacement=sim.get("displacement"),
+                        stress_corotational=sim.get("stress_corotational"),
+                        state=sim.get("state"), damage_index=sim.get("damage_index"))
+    sim.close()
+
+    # one plastic JC step (jc_thermal_units_test.cpp:9-20) in both heat-unit conventions
+    out = {}
+    for tag, w2h in (("legacy", 1.0), ("scaled", 1.0e6)):
+        props = np.array(REFERENCE_JC_PROPS[:13] + (w2h,))
+        first = O.vumat_block(O.oracle_lib(), props, 2.5e-5, np.zeros((1, 6)), np.zeros((1, 6)),
+                              np.zeros((1, 6)), np.array([293.0]), np.zeros(1), np.zeros(1))
+        inc = np.zeros((1, 6))
+        inc[0, 0] = 400 * 2.5e-5
+        second = O.vumat_block(O.oracle_lib(), props, 2.5e-5, inc, first["stress"], first["state"],
+                               first["temperature"], first["energy_internal"],
+                               first["energy_inelastic"])
+        for k, v in second.items():
+            out[f"{tag}_{k}"] = v
+    np.savez_compressed(os.path.join(HERE, "ref_jc_thermal.npz"), **out)
+    print("fixtures written to", HERE)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")

@@ -1,0 +1,181 @@
+"""The CPU oracle pinned before it is trusted: against the reference's archived run, against
+the reference library itself (compiled from its sources into oracle/_ref), and against the
+reference's own known-answer tests restated here."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import golden, load_golden_timeseries, max_rel
+
+import oracle as O
+from vpd.case import REFERENCE_JC_PROPS, Case, pd_coarse, tensile_bar
+
+
+def test_oracle_reproduces_archived_pd_coarse():
+    """benchmarks/tensile3d/raw/pd_coarse: all 4800 steps, every timeseries column and the
+    final nodal fields. The archive was written by gfortran's JC; the restated JC and the
+    restated increment agree to its 16-digit print precision."""
+    header, g = load_golden_timeseries()
+    sim = O.OracleSim(pd_coarse())
+    rows = sim.step(4800)
+    mine = rows[g[:, 0].astype(int) - 1]
+    for j, name in enumerate(header):
+        assert max_rel(mine[:, j], g[:, j]) < 1e-12, name
+    snap = np.load(golden("pd_coarse_snapshot.npz"))
+    assert max_rel(sim.get("displacement"), snap["displacement"]) < 1e-13
+    assert max_rel(sim.get("velocity"), snap["velocity"]) < 1e-12
+    assert max_rel(sim.get("stress_spatial")[:, 0], snap["axial_stress"]) < 1e-12
+    assert max_rel(sim.get("state")[:, 1], snap["eqps"]) < 1e-12
+
+
+def test_oracle_matches_reference_library_fixture():
+    """The reference library's run of the jittered, damaged 40x10x10 bar (fixture) is
+    reproduced bit for bit."""
+    ref = np.load(golden("ref_tensile_bar_1.npz"))
+    bar = tensile_bar(1, jitter=0.05, jitter_seed=7, damage_mode=1, damage_initiation=0.004)
+    sim = O.OracleSim(bar)
+    diag = sim.step(300)
+    assert np.array_equal(diag, ref["diag"])
+    assert np.array_equal(sim.get("displacement"), ref["displacement"])
+    assert np.array_equal(sim.get("stress_corotational"), ref["stress_corotational"])
+    assert np.array_equal(sim.get("state"), ref["state"])
+    assert np.array_equal(sim.get("damage_index"), ref["damage_index"])
+
+
+@pytest.mark.skipif(not O.reference_available(), reason="reference library not built")
+def test_oracle_matches_reference_library_live():
+    case = pd_coarse().replace(steps=200)
+    a, b = O.OracleSim(case), O.RefSim(case)
+    assert np.array_equal(a.step(200), b.step(200))
+    for field in ("displacement", "velocity", "stress_corotational", "state", "force_density"):
+        assert np.array_equal(a.get(field), b.get(field)), field
+
+
+def test_neighbor_lattice_regression():
+    """tests/neighbor_lattice_regression.cpp: 9^3 lattices, h in {2/3, 1, 2}, shifted; the
+    list equals the integer-lattice neighbourhood d^2 in (0, 9], in ascending order."""
+    n = 9
+    ijk = np.stack(np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij"), -1).reshape(-1, 3)
+    d2 = ((ijk[:, None, :] - ijk[None, :, :]) ** 2).sum(-1)
+    for h in (2.0 / 3.0, 1.0, 2.0):
+        for shift in (0.0, -123.456, 10000.125):
+            row_ptr, col = O.neighbor_list(shift + ijk * h, 3 * h)
+            for p in range(n ** 3):
+                expected = np.nonzero((d2[p] > 0) & (d2[p] <= 9))[0]
+                assert np.array_equal(col[row_ptr[p]:row_ptr[p + 1]], expected)
+
+
+def test_neighbor_list_matches_reference_fixture():
+    ref = np.load(golden("ref_neighbors_jittered.npz"))
+    row_ptr, col = O.neighbor_list(ref["positions"], float(ref["horizon"]))
+    assert np.array_equal(row_ptr, ref["row_ptr"]) and np.array_equal(col, ref["col"])
+
+
+def test_affine_completeness():
+    """tests/correspondence_sampling_test.cpp: total volume 512; an affine field gives the
+    exact F at every node, boundary nodes included."""
+    case = Case(name="cube", nx=9, ny=9, nz=9, spacing=1.0, horizon=2.0, dt=1e-5, steps=1,
+                density=1.0, props=REFERENCE_JC_PROPS, grip_velocity=1.0, ramp_time=1.0)
+    sim = O.OracleSim(case)
+    x, vol = sim.get("position"), sim.get("volume")[:, 0]
+    assert abs(vol.sum() - 512.0) < 1e-12
+    row_ptr, col = sim.neighbors()
+    rc, kinv = O.shape_inverse(x, vol, row_ptr, col)
+    assert rc == 0
+    u = np.stack([0.02 * x[:, 0] + 0.03 * x[:, 1], -0.01 * x[:, 1], 0.04 * x[:, 2]], 1)
+    F = O.deformation(x, u, vol, row_ptr, col, kinv)
+    expected = np.array([1.02, 0.03, 0, 0, 0.99, 0, 0, 0, 1.04])
+    assert np.max(np.abs(F - expected)) < 1e-12
+
+
+def test_corotational_known_answers():
+    """tests/corotational_kinematics_test.cpp: rigid rotation gives zero D-bar; F=diag(1.01)
+    at dt=0.01 gives D-bar_11=1 and V_11=1.01; E_11=0.01005; finite spin matches exp."""
+    I = np.eye(3).reshape(1, 9)
+    a = 1e-7
+    R = np.array([[np.cos(a), -np.sin(a), 0, np.sin(a), np.cos(a), 0, 0, 0, 1.0]])
+    rc, out = O.corotational(I, R, I, I, 1.0)
+    assert rc == 0 and np.max(np.abs(out["rate_of_deformation"])) < 1e-13
+    assert np.max(np.abs(out["left_stretch"] - I)) < 1e-13
+    F = np.array([[1.01, 0, 0, 0, 1, 0, 0, 0, 1.0]])
+    rc, out = O.corotational(I, F, I, I, 0.01)
+    assert abs(out["rate_of_deformation"][0, 0] - 1.0) < 1e-12
+    assert abs(out["left_stretch"][0, 0] - 1.01) < 1e-12
+    assert abs(out["strain"][0, 0] - 0.01005) < 1e-12
+    for axis in range(3):
+        for angle in (1e-7, 0.01, 0.1, 0.7, -0.4):
+            ia, ib = (axis + 1) % 3, (axis + 2) % 3
+            f = np.eye(3)
+            f[ia, ib], f[ib, ia] = -angle, angle
+            e = np.eye(3)
+            e[ia, ia] = e[ib, ib] = np.cos(angle)
+            e[ia, ib], e[ib, ia] = -np.sin(angle), np.sin(angle)
+            rc, out = O.corotational(I, f.reshape(1, 9), I, I, 1.0)
+            assert np.max(np.abs(out["rotation"] - e.reshape(1, 9))) < 2e-14
+
+
+def test_jc_thermal_units():
+    """tests/jc_thermal_units_test.cpp: workToHeat 1 vs 1e6 gives identical first-step stress
+    and a temperature rise in ratio 1e6; the values are the fixture's."""
+    ref = np.load(golden("ref_jc_thermal.npz"))
+    out = {}
+    for tag, w2h in (("legacy", 1.0), ("scaled", 1.0e6)):
+        props = np.array(REFERENCE_JC_PROPS[:13] + (w2h,))
+        first = O.vumat_block(O.oracle_lib(), props, 2.5e-5, np.zeros((1, 6)), np.zeros((1, 6)),
+                              np.zeros((1, 6)), np.array([293.0]), np.zeros(1), np.zeros(1))
+        inc = np.zeros((1, 6))
+        inc[0, 0] = 400 * 2.5e-5
+        out[tag] = O.vumat_block(O.oracle_lib(), props, 2.5e-5, inc, first["stress"],
+                                 first["state"], first["temperature"], first["energy_internal"],
+                                 first["energy_inelastic"])
+        for k, v in out[tag].items():
+            assert np.array_equal(v, ref[f"{tag}_{k}"])
+    assert np.max(np.abs(out["legacy"]["stress"] - out["scaled"]["stress"])) < 1e-10
+    da, db = out["legacy"]["temperature"][0] - 293, out["scaled"]["temperature"][0] - 293
+    assert da > 0 and abs(db / (1e6 * da) - 1) < 1e-6
+
+
+def test_critical_stretch_known_answer():
+    """tests/outer_damage_test.cpp:61-90: two points, stretch 0.1 > 0.05 breaks both directed
+    bonds; no healing on unloading; the compression threshold is honoured."""
+    pos = np.array([[0.0, 0, 0], [1.0, 0, 0]])
+    vol = np.array([1.0, 2.0])
+    row_ptr, col = np.array([0, 1, 2]), np.array([1, 0], dtype=np.int32)
+    disp = np.array([[0.0, 0, 0], [0.10, 0, 0]])
+    rc, bd, idx = O.damage(pos, disp, vol, row_ptr, col, 0.05, 0.0, np.zeros(2))
+    assert rc == 0 and np.array_equal(bd, [1, 1]) and np.array_equal(idx, [1, 1])
+    rc, bd2, _ = O.damage(pos, np.zeros((2, 3)), vol, row_ptr, col, 0.05, 0.0, bd)
+    assert np.array_equal(bd2, [1, 1])
+    disp = np.array([[0.0, 0, 0], [-0.03, 0, 0]])
+    rc, bd3, _ = O.damage(pos, disp, vol, row_ptr, col, 0.05, 0.02, np.zeros(2))
+    assert bd3[0] == 1.0
+
+
+REF_TESTS = ("neighbor_lattice_regression", "neighbor_search_test", "correspondence_sampling_test",
+             "corotational_kinematics_test", "outer_damage_test", "observation_window_test",
+             "json_numeric_test")
+
+
+@pytest.mark.parametrize("name", REF_TESTS)
+def test_reference_unit_tests_pass_on_the_built_library(name):
+    """The reference's own unit tests, compiled from its sources against the library the
+    oracle is pinned to (oracle/_ref), pass."""
+    exe = os.path.join(O.REF_DIR, name)
+    if not os.path.exists(exe):
+        pytest.skip("reference tests not built")
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=120,
+                       env=dict(os.environ, OMP_NUM_THREADS="2"))
+    assert r.returncode == 0, r.stdout + r.stderr
+
+
+def test_reference_interface_contract_with_restated_probe():
+    """tests/interface_contract_test.cpp through the reference adapter and the restated
+    ContractProbe plugin: packing, padding, 1/255/256/257/513 rows, two-step history."""
+    exe = os.path.join(O.REF_DIR, "interface_contract_test")
+    if not os.path.exists(exe):
+        pytest.skip("reference tests not built")
+    r = subprocess.run([exe, os.path.join(O.REF_DIR, "contract_probe_plugin.so")],
+                       capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stdout + r.stderr

@@ -1,0 +1,732 @@
+// C ABI of libvpd_gpu.so: the simulation handle (create / step / download / destroy).
+//
+// vpd_create mirrors runMaterial's set-up (src/host/BoundaryValueCaseRunner.cpp:142-190):
+// the lattice of makeParticlePatch (src/host/Geometry.cpp:10-34) generated on the device,
+// the sorted neighbour lists, K^-1, the boundary bands, pins and observation weights
+// (src/host/ParticleSets.cpp:12-71, src/host/BoundaryConditions.cpp:54-68,96-110,
+// include/ObservationWindow.hpp:13-56), the initial material state and the constraints at
+// t = 0. vpd_step runs the step loop (:207-306) as device kernels, captured in a CUDA graph.
+#include "vpd_math.cuh"
+#include "vpd_step.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <string>
+#include <vector>
+
+namespace vpd {
+
+thread_local std::string g_error;
+
+int set_error(int status, const std::string &message) {
+  g_error = message;
+  return status;
+}
+int cuda_error(cudaError_t e, const char *what) {
+  return set_error(VPD_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// Position generator: the lattice of makeParticlePatch plus the seeded jitter, every
+// operation rounded as the host formula (no FMA contraction) so hosts reproduce it exactly.
+__device__ __forceinline__ uint64_t splitmix64(uint64_t x) {
+  x += 0x9E3779B97F4A7C15ull;
+  uint64_t z = x;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+struct LatticeParams {
+  int nx, ny, nz;
+  double h, yoff, zoff, volume, amp;
+  uint64_t seed;
+  int jitter;
+};
+
+__global__ void k_lattice(LatticeParams L, double4 *xv) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t n = (int64_t)L.nx * L.ny * L.nz;
+  if (p >= n)
+    return;
+  const int k = (int)(p % L.nz), j = (int)((p / L.nz) % L.ny), i = (int)(p / ((int64_t)L.ny * L.nz));
+  double x[3] = {__dmul_rn((double)i, L.h), __dsub_rn(__dmul_rn((double)j, L.h), L.yoff),
+                 __dsub_rn(__dmul_rn((double)k, L.h), L.zoff)};
+  if (L.jitter) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const uint64_t r =
+          splitmix64(L.seed ^ (0xD1B54A32D192ED03ull * (uint64_t)(3 * p + d + 1)));
+      const double u = (double)(r >> 11) * 0x1.0p-53;
+      x[d] = __dadd_rn(x[d], __dmul_rn(__dadd_rn(2.0 * u, -1.0), L.amp));
+    }
+  }
+  const double v = L.volume * ((i == 0 || i == L.nx - 1) ? 0.5 : 1.0) *
+                   ((j == 0 || j == L.ny - 1) ? 0.5 : 1.0) * ((k == 0 || k == L.nz - 1) ? 0.5 : 1.0);
+  xv[p] = make_double4(x[0], x[1], x[2], v);
+}
+
+__global__ void k_pack_xv(const double *pos, const double *vol, int64_t n, double4 *xv) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n)
+    xv[i] = make_double4(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], vol[i]);
+}
+
+// Volume-weighted broken-bond fraction (damageIndex, PdSimpleDamage.cpp:23-36).
+__global__ void k_damage_index(int64_t n, const double4 *xv, const int32_t *len,
+                               const int64_t *slice_off, const int32_t *sell,
+                               const uint32_t *words, double *out) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n)
+    return;
+  const int64_t s = i >> 5, off = slice_off[s];
+  const int lane = (int)(i & 31);
+  double damaged = 0.0, total = 0.0;
+  for (int k = 0; k < len[i]; ++k) {
+    const double v = xv[sell[off + 32 * k + lane]].w;
+    if ((words[(off >> 5) + k] >> lane) & 1u)
+      damaged += v;
+    total += v;
+  }
+  out[i] = total > 0.0 ? damaged / total : 0.0;
+}
+
+// ------------------------------------------------------------------ host-side sets
+struct Sets {
+  std::vector<uint8_t> flags;
+  std::vector<double> obsw;
+  double interior = 0, gauge = 0, lat_gauge = 0, area = 0, n_lat_pos = 0, n_lat_neg = 0;
+  int axis = 0, lateral = 1;
+};
+
+// selectBoundaryRegion (ParticleSets.cpp:12-50)
+static bool select_region(const std::vector<double> &x, int64_t n, int comp, bool selectMin,
+                          double width, std::vector<uint8_t> &flags, uint8_t bit) {
+  double extreme = selectMin ? std::numeric_limits<double>::infinity()
+                             : -std::numeric_limits<double>::infinity();
+  for (int64_t i = 0; i < n; ++i)
+    extreme = selectMin ? std::min(extreme, x[3 * i + comp]) : std::max(extreme, x[3 * i + comp]);
+  const double tol = 1.0e-10 * std::max(1.0, std::abs(extreme));
+  bool any = false;
+  for (int64_t i = 0; i < n; ++i) {
+    const double dist = selectMin ? x[3 * i + comp] - extreme : extreme - x[3 * i + comp];
+    if (dist <= width + tol) {
+      flags[i] |= bit;
+      any = true;
+    }
+  }
+  return any;
+}
+
+static int build_sets(const vpd_case &c, const std::vector<double> &x, const std::vector<double> &vol,
+                      Sets &s) {
+  const int64_t n = (int64_t)vol.size();
+  const double h = c.spacing;
+  s.axis = c.load_axis;
+  s.lateral = s.axis == 0 ? 1 : 0;
+  s.flags.assign((size_t)n, 0);
+  s.obsw.assign((size_t)n, 0.0);
+  const double width = (double)(c.region_layers - 1) * h + 1.0e-9 * h;
+  if (!select_region(x, n, s.axis, true, width, s.flags, FLAG_SUPPORT) ||
+      !select_region(x, n, s.axis, false, width, s.flags, FLAG_LOADED))
+    return set_error(VPD_ERR_INVALID, "Boundary-region selection returned no particles.");
+  // anchor: support point closest to the centroid (BoundaryConditions.cpp:58-67)
+  double centre[3] = {0, 0, 0};
+  for (int64_t i = 0; i < n; ++i)
+    for (int d = 0; d < 3; ++d)
+      centre[d] += x[3 * i + d];
+  for (double &v : centre)
+    v /= (double)n;
+  int64_t anchor = -1;
+  double best = std::numeric_limits<double>::infinity();
+  for (int64_t i = 0; i < n; ++i)
+    if (s.flags[i] & FLAG_SUPPORT) {
+      double dist = 0.0;
+      for (int d = 0; d < 3; ++d) {
+        const double delta = x[3 * i + d] - centre[d];
+        dist += delta * delta;
+      }
+      if (dist < best)
+        best = dist, anchor = i;
+    }
+  if (anchor < 0)
+    return set_error(VPD_ERR_INVALID, "Closest-particle selection requires candidates.");
+  int64_t pin = anchor;
+  double greatestY = -1.0e100;
+  for (int64_t i = 0; i < n; ++i)
+    if (s.flags[i] & FLAG_SUPPORT) {
+      if (std::abs(x[3 * i] - x[3 * anchor]) < 1e-8 && std::abs(x[3 * i + 2] - x[3 * anchor + 2]) < 1e-8 &&
+          x[3 * i + 1] > greatestY)
+        greatestY = x[3 * i + 1], pin = i;
+    }
+  s.flags[anchor] |= FLAG_ANCHOR;
+  s.flags[pin] |= FLAG_ROTATION_PIN;
+  double sl = 0, ss = 0, nl = 0, ns = 0;
+  for (int64_t i = 0; i < n; ++i) {
+    if (s.flags[i] & FLAG_LOADED) sl += x[3 * i + s.axis], nl += 1;
+    if (s.flags[i] & FLAG_SUPPORT) ss += x[3 * i + s.axis], ns += 1;
+  }
+  s.gauge = std::abs(sl / nl - ss / ns);
+  select_region(x, n, s.lateral, true, 1.0e-9 * h, s.flags, FLAG_LATERAL_NEG);
+  select_region(x, n, s.lateral, false, 1.0e-9 * h, s.flags, FLAG_LATERAL_POS);
+  double sp = 0, sn = 0;
+  for (int64_t i = 0; i < n; ++i) {
+    if (s.flags[i] & FLAG_LATERAL_POS) sp += x[3 * i + s.lateral], s.n_lat_pos += 1;
+    if (s.flags[i] & FLAG_LATERAL_NEG) sn += x[3 * i + s.lateral], s.n_lat_neg += 1;
+  }
+  s.lat_gauge = std::abs(sp / s.n_lat_pos - sn / s.n_lat_neg);
+  // observation window (ObservationWindow.hpp:13-56)
+  double lo = x[s.axis], hi = lo;
+  for (int64_t i = 0; i < n; ++i)
+    lo = std::min(lo, x[3 * i + s.axis]), hi = std::max(hi, x[3 * i + s.axis]);
+  const double band = (double)(c.region_layers - 1) * h;
+  const double a = std::isnan(c.observation_min) ? lo + band : c.observation_min;
+  const double b = std::isnan(c.observation_max) ? hi - band : c.observation_max;
+  if (!std::isfinite(a) || !std::isfinite(b) || a < lo || b > hi || a >= b)
+    return set_error(VPD_ERR_INVALID,
+                     "Observation window must lie within the body and have positive length.");
+  const double tol = 1e-8 * h;
+  bool foundA = false, foundB = false;
+  for (int64_t i = 0; i < n; ++i) {
+    const double v = x[3 * i + s.axis];
+    const bool atA = std::abs(v - a) < tol, atB = std::abs(v - b) < tol;
+    foundA = foundA || atA;
+    foundB = foundB || atB;
+    if (v < a - tol || v > b + tol)
+      continue;
+    const bool interiorEnd = (atA && a > lo + tol) || (atB && b < hi - tol);
+    s.obsw[i] = vol[i] * (interiorEnd ? 0.5 : 1.0);
+    s.interior += s.obsw[i];
+  }
+  if (!foundA || !foundB)
+    return set_error(VPD_ERR_INVALID, "Observation bounds must coincide with reference nodal planes.");
+  const int cross = s.axis == 0 ? c.ny : c.nx;
+  s.area = (double)((cross - 1) * (c.nz - 1)) * h * h;
+  return VPD_OK;
+}
+
+}  // namespace vpd
+
+using namespace vpd;
+
+struct vpd_handle {
+  vpd_case c{};
+  int64_t n = 0, nbonds = 0, sell_total = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaGraphExec_t graph = nullptr;
+  int graph_steps = 0;
+  float last_ms = 0.0f;
+  int64_t step = 0;  // increments completed
+  std::vector<void *> allocations;
+  double4 *xv = nullptr, *u0 = nullptr, *u1 = nullptr, *vel = nullptr, *acc = nullptr, *force = nullptr;
+  int64_t *row_ptr = nullptr, *slice_off = nullptr, *step_dev = nullptr;
+  int32_t *col = nullptr, *len = nullptr, *sell = nullptr;
+  uint32_t *words = nullptr;
+  double *kinv = nullptr, *F = nullptr, *Fn = nullptr, *Vn = nullptr, *Rn = nullptr, *En = nullptr;
+  double *sig = nullptr, *state = nullptr, *eI = nullptr, *eP = nullptr, *M = nullptr, *obsw = nullptr;
+  double *part_mat = nullptr, *part_force = nullptr, *accum = nullptr, *diag = nullptr;
+  uint8_t *flags = nullptr;
+  unsigned *status_dev = nullptr, *counter = nullptr;
+  StepParams params{};
+};
+
+namespace {
+
+template <typename T> int dalloc(vpd_handle *h, T **p, size_t count) {
+  void *q = nullptr;
+  VPD_CUDA(cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T)));
+  h->allocations.push_back(q);
+  *p = static_cast<T *>(q);
+  return VPD_OK;
+}
+
+int check_case(const vpd_case *c) {
+  if (!c)
+    return set_error(VPD_ERR_INVALID, "case is NULL");
+  if (c->nx < 2 || c->ny < 2 || c->nz < 2)
+    return set_error(VPD_ERR_INVALID, "PD patch geometry requires nx/ny/nz >= 2.");
+  if (!(c->spacing > 0.0) || !(c->horizon > 0.0))
+    return set_error(VPD_ERR_INVALID, "PD geometry requires positive spacing and horizon.");
+  if (!(c->dt > 0.0) || !std::isfinite(c->dt))
+    return set_error(VPD_ERR_INVALID, "time_integration requires dt > 0.");
+  if (!(c->density > 0.0))
+    return set_error(VPD_ERR_INVALID, "Explicit dynamics requires density > 0.");
+  if (c->nstatev < 6 || c->nstatev > 64)
+    return set_error(VPD_ERR_INVALID, "JohnsonCook VUMAT requires 6 <= nstatev <= 64");
+  if (c->region_layers < 1 || (c->load_axis != 0 && c->load_axis != 1))
+    return set_error(VPD_ERR_INVALID, "regional loading needs regionLayers >= 1 and axis x or y");
+  if (c->bc_mode == VPD_BC_SMOOTH_DISPLACEMENT) {
+    if (c->amplitude == 0.0 || !(c->rise_time > 0.0))
+      return set_error(VPD_ERR_INVALID, "smooth displacement needs amplitude != 0 and riseTime > 0");
+  } else if (c->bc_mode == VPD_BC_VELOCITY_RAMP) {
+    if (c->grip_velocity == 0.0 || !(c->ramp_time > 0.0))
+      return set_error(VPD_ERR_INVALID, "velocity ramp needs grip_velocity != 0 and ramp_time > 0");
+  } else {
+    return set_error(VPD_ERR_INVALID, "unknown boundary-condition mode");
+  }
+  if (c->damage_mode == VPD_DAMAGE_CRITICAL_STRETCH && !(c->damage_initiation > 0.0))
+    return set_error(VPD_ERR_INVALID, "critical_stretch requires initiation > 0.");
+  if (c->damage_mode != VPD_DAMAGE_NONE && c->damage_mode != VPD_DAMAGE_CRITICAL_STRETCH)
+    return set_error(VPD_ERR_INVALID, "unknown damage mode");
+  if (c->precision != VPD_PRECISION_FP64)
+    return set_error(VPD_ERR_UNSUPPORTED, "this build implements the FP64 precision mode only");
+  if (c->material_mode != VPD_MATERIAL_VUMAT)
+    return set_error(VPD_ERR_UNSUPPORTED, "this build implements the plain VUMAT material only");
+  for (int k = 0; k < 14; ++k)
+    if (!std::isfinite(c->props[k]))
+      return set_error(VPD_ERR_INVALID, "Johnson-Cook props must be finite");
+  return VPD_OK;
+}
+
+int read_status(vpd_handle *h) {
+  unsigned st = 0;
+  VPD_CUDA(cudaMemcpyAsync(&st, h->status_dev, sizeof st, cudaMemcpyDeviceToHost, h->stream));
+  VPD_CUDA(cudaStreamSynchronize(h->stream));
+  if (st & STATUS_SINGULAR_K)
+    return set_error(VPD_ERR_SINGULAR, "Singular tensor in PD shape tensor.");
+  if (st & STATUS_SINGULAR_F)
+    return set_error(VPD_ERR_SINGULAR, "Invalid deformation gradient determinant.");
+  if (st & STATUS_SINGULAR_KINEMATICS)
+    return set_error(VPD_ERR_SINGULAR, "Corotational update encountered a singular tensor.");
+  return VPD_OK;
+}
+
+int create_impl(vpd_handle *h, const vpd_case *c, const double *positions, const double *volumes) {
+  int rc = check_case(c);
+  if (rc)
+    return rc;
+  h->c = *c;
+  const int64_t n = (int64_t)c->nx * c->ny * c->nz;
+  if (n > INT32_MAX)
+    return set_error(VPD_ERR_CAPACITY, "more than 2^31 points");
+  h->n = n;
+
+  // nominal lattice on the host: bands, pins and observation weights (all host-side checks
+  // finish before the first CUDA call)
+  const double hsp = c->spacing;
+  const double yoff = 0.5 * (double)(c->ny - 1) * hsp, zoff = 0.5 * (double)(c->nz - 1) * hsp;
+  const double volume = hsp * hsp * hsp;
+  std::vector<double> nominal((size_t)(3 * n)), vol((size_t)n);
+  {
+    int64_t p = 0;
+    for (int i = 0; i < c->nx; ++i)
+      for (int j = 0; j < c->ny; ++j)
+        for (int k = 0; k < c->nz; ++k, ++p) {
+          nominal[3 * p] = (double)i * hsp;
+          nominal[3 * p + 1] = (double)j * hsp - yoff;
+          nominal[3 * p + 2] = (double)k * hsp - zoff;
+          vol[p] = volume * ((i == 0 || i == c->nx - 1) ? 0.5 : 1.0) *
+                   ((j == 0 || j == c->ny - 1) ? 0.5 : 1.0) * ((k == 0 || k == c->nz - 1) ? 0.5 : 1.0);
+        }
+  }
+  Sets sets;
+  if ((rc = build_sets(*c, nominal, vol, sets)))
+    return rc;
+  VPD_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+  VPD_CUDA(cudaEventCreate(&h->ev0));
+  VPD_CUDA(cudaEventCreate(&h->ev1));
+  cudaStream_t s = h->stream;
+
+  // device arrays
+  if ((rc = dalloc(h, &h->xv, n)) || (rc = dalloc(h, &h->u0, n)) || (rc = dalloc(h, &h->u1, n)) ||
+      (rc = dalloc(h, &h->vel, n)) || (rc = dalloc(h, &h->acc, n)) || (rc = dalloc(h, &h->force, n)) ||
+      (rc = dalloc(h, &h->kinv, 9 * n)) || (rc = dalloc(h, &h->F, 9 * n)) ||
+      (rc = dalloc(h, &h->Fn, 9 * n)) || (rc = dalloc(h, &h->Vn, 9 * n)) ||
+      (rc = dalloc(h, &h->Rn, 9 * n)) || (rc = dalloc(h, &h->En, 6 * n)) ||
+      (rc = dalloc(h, &h->sig, 6 * n)) || (rc = dalloc(h, &h->state, (size_t)c->nstatev * n)) ||
+      (rc = dalloc(h, &h->eI, n)) || (rc = dalloc(h, &h->eP, n)) || (rc = dalloc(h, &h->M, 9 * n)) ||
+      (rc = dalloc(h, &h->obsw, n)) || (rc = dalloc(h, &h->flags, n)) ||
+      (rc = dalloc(h, &h->row_ptr, n + 1)) || (rc = dalloc(h, &h->step_dev, 1)) ||
+      (rc = dalloc(h, &h->status_dev, 1)) || (rc = dalloc(h, &h->counter, 1)) ||
+      (rc = dalloc(h, &h->accum, ACC_COUNT)) || (rc = dalloc(h, &h->diag, (size_t)kDiagRing * VPD_DIAG_COLS)))
+    return rc;
+  VPD_CUDA(cudaMemsetAsync(h->u0, 0, sizeof(double4) * n, s));
+  VPD_CUDA(cudaMemsetAsync(h->status_dev, 0, sizeof(unsigned), s));
+  VPD_CUDA(cudaMemsetAsync(h->counter, 0, sizeof(unsigned), s));
+
+  // positions
+  if (positions) {
+    double *dpos = nullptr, *dvol = nullptr;
+    VPD_CUDA(cudaMalloc(&dpos, sizeof(double) * 3 * n));
+    VPD_CUDA(cudaMalloc(&dvol, sizeof(double) * n));
+    VPD_CUDA(cudaMemcpyAsync(dpos, positions, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s));
+    VPD_CUDA(cudaMemcpyAsync(dvol, volumes ? volumes : vol.data(), sizeof(double) * n,
+                             cudaMemcpyHostToDevice, s));
+    k_pack_xv<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(dpos, dvol, n, h->xv);
+    VPD_CUDA(cudaStreamSynchronize(s));
+    cudaFree(dpos);
+    cudaFree(dvol);
+  } else {
+    LatticeParams L{c->nx, c->ny, c->nz, hsp, yoff, zoff, volume, c->jitter * hsp, c->jitter_seed,
+                    c->jitter != 0.0};
+    k_lattice<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(L, h->xv);
+  }
+  VPD_CUDA(cudaMemcpyAsync(h->flags, sets.flags.data(), n, cudaMemcpyHostToDevice, s));
+  VPD_CUDA(cudaMemcpyAsync(h->obsw, sets.obsw.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s));
+
+  // neighbour lists: sorted CSR, then the sliced-ELL copy the kernels stream
+  {
+    NeighborScratch scr;
+    NeighborGrid grid;
+    if ((rc = neighbor_scratch_alloc(scr, n)) == VPD_OK &&
+        (rc = neighbor_count(h->xv, n, c->horizon, h->row_ptr, grid, scr, s)) == VPD_OK) {
+      VPD_CUDA(cudaMemcpyAsync(&h->nbonds, h->row_ptr + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+      VPD_CUDA(cudaStreamSynchronize(s));
+      if ((rc = dalloc(h, &h->col, (size_t)h->nbonds)) == VPD_OK)
+        rc = neighbor_fill(h->xv, n, h->row_ptr, h->col, grid, scr, s);
+    }
+    neighbor_scratch_free(scr);
+    if (rc)
+      return rc;
+  }
+  if ((rc = build_sell(h->row_ptr, h->col, n, &h->len, &h->slice_off, &h->sell, &h->sell_total, s)))
+    return rc;
+  h->allocations.push_back(h->len);
+  h->allocations.push_back(h->slice_off);
+  h->allocations.push_back(h->sell);
+  if ((rc = dalloc(h, &h->words, (size_t)(h->sell_total / 32))))
+    return rc;
+  VPD_CUDA(cudaMemsetAsync(h->words, 0, sizeof(uint32_t) * std::max<int64_t>(h->sell_total / 32, 1), s));
+  const int mat_blocks = material_grid(n);
+  const int force_blocks = (int)(((n + 31) / 32 * 32 + kBondThreads - 1) / kBondThreads);
+  if ((rc = dalloc(h, &h->part_mat, (size_t)mat_blocks * PM_COUNT)) ||
+      (rc = dalloc(h, &h->part_force, (size_t)force_blocks * PF_COUNT)))
+    return rc;
+
+  // step parameters
+  StepParams &p = h->params;
+  p.n = n;
+  p.dt = c->dt;
+  p.rho = c->density;
+  p.xv = h->xv, p.len = h->len, p.slice_off = h->slice_off, p.sell = h->sell, p.words = h->words;
+  p.u0 = h->u0, p.u1 = h->u1, p.vel = h->vel, p.acc = h->acc, p.force = h->force;
+  p.kinv = h->kinv, p.F = h->F, p.Fn = h->Fn, p.Vn = h->Vn, p.Rn = h->Rn, p.En = h->En;
+  p.sig = h->sig, p.state = h->state, p.eI = h->eI, p.eP = h->eP, p.M = h->M;
+  p.nstatev = c->nstatev;
+  p.flags = h->flags, p.obsw = h->obsw;
+  p.jc = make_jc_params(c->props);
+  p.bc = BcParams{c->bc_mode, c->amplitude, c->rise_time, c->grip_velocity, c->ramp_time,
+                  sets.axis, sets.lateral, c->plane_strain};
+  p.damage = c->damage_mode == VPD_DAMAGE_CRITICAL_STRETCH;
+  p.dmg_initiation = c->damage_initiation;
+  p.dmg_failure = c->damage_failure;
+  p.use_compression = c->damage_failure > 0.0 && std::isfinite(c->damage_failure);
+  p.tension2 = (1.0 + c->damage_initiation) * (1.0 + c->damage_initiation);
+  p.compression2 = c->damage_failure < 1.0 ? (1.0 - c->damage_failure) * (1.0 - c->damage_failure) : 0.0;
+  p.step = h->step_dev, p.status = h->status_dev;
+  p.part_mat = h->part_mat, p.part_force = h->part_force, p.accum = h->accum, p.diag = h->diag;
+  p.counter = h->counter;
+  p.mat_blocks = mat_blocks;
+  p.interior = sets.interior, p.gauge = sets.gauge, p.lat_gauge = sets.lat_gauge;
+  p.area = sets.area, p.n_lat_pos = sets.n_lat_pos, p.n_lat_neg = sets.n_lat_neg;
+  p.sign = (c->bc_mode == VPD_BC_SMOOTH_DISPLACEMENT ? c->amplitude : c->grip_velocity) > 0.0 ? 1.0 : -1.0;
+
+  if ((rc = launch_shape_inverse_sell(p, s)))
+    return rc;
+  if ((rc = launch_init(p, s)))
+    return rc;
+  const double acc0[ACC_COUNT] = {0.0, 0.0, 0.0, 1.0};
+  const int64_t one = 1;
+  VPD_CUDA(cudaMemcpyAsync(h->accum, acc0, sizeof acc0, cudaMemcpyHostToDevice, s));
+  VPD_CUDA(cudaMemcpyAsync(h->step_dev, &one, sizeof one, cudaMemcpyHostToDevice, s));
+  return read_status(h);
+}
+
+void destroy_impl(vpd_handle *h) {
+  if (h->graph)
+    cudaGraphExecDestroy(h->graph);
+  if (h->stream)
+    cudaStreamSynchronize(h->stream);
+  for (void *p : h->allocations)
+    cudaFree(p);
+  if (h->ev0)
+    cudaEventDestroy(h->ev0);
+  if (h->ev1)
+    cudaEventDestroy(h->ev1);
+  if (h->stream)
+    cudaStreamDestroy(h->stream);
+  delete h;
+}
+
+constexpr int kGraphSteps = 8;
+
+int ensure_graph(vpd_handle *h) {
+  if (h->graph)
+    return VPD_OK;
+  cudaGraph_t g = nullptr;
+  VPD_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+  int rc = VPD_OK;
+  for (int k = 0; k < kGraphSteps && rc == VPD_OK; ++k)
+    rc = launch_increment(h->params, h->stream);
+  cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+  if (rc)
+    return rc;
+  if (e != cudaSuccess)
+    return cuda_error(e, "cudaStreamEndCapture");
+  e = cudaGraphInstantiate(&h->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess)
+    return cuda_error(e, "cudaGraphInstantiate");
+  h->graph_steps = kGraphSteps;
+  return VPD_OK;
+}
+
+int copy_rows(vpd_handle *h, int64_t first_step, int64_t count, double *out) {
+  // rows of increments first_step .. first_step+count-1 sit at (step-1) % ring
+  int64_t done = 0;
+  while (done < count) {
+    const int64_t slot = (first_step - 1 + done) % kDiagRing;
+    const int64_t m = std::min<int64_t>(count - done, kDiagRing - slot);
+    VPD_CUDA(cudaMemcpyAsync(out + done * VPD_DIAG_COLS, h->diag + slot * VPD_DIAG_COLS,
+                             sizeof(double) * VPD_DIAG_COLS * m, cudaMemcpyDeviceToHost, h->stream));
+    done += m;
+  }
+  return VPD_OK;
+}
+
+template <typename Fn> int with_host_buffer(size_t count, Fn &&fn) {
+  std::vector<double> buf(count);
+  return fn(buf);
+}
+
+}  // namespace
+
+extern "C" {
+
+int vpd_abi_version(void) { return VPD_ABI_VERSION; }
+const char *vpd_last_error(void) { return g_error.c_str(); }
+
+int vpd_field_width(const vpd_handle *h, int field) {
+  switch (field) {
+  case VPD_FIELD_VOLUME: case VPD_FIELD_TEMPERATURE: case VPD_FIELD_ENERGY_INTERNAL:
+  case VPD_FIELD_ENERGY_INELASTIC: case VPD_FIELD_DAMAGE_INDEX:
+    return 1;
+  case VPD_FIELD_POSITION: case VPD_FIELD_DISPLACEMENT: case VPD_FIELD_VELOCITY:
+  case VPD_FIELD_ACCELERATION: case VPD_FIELD_FORCE_DENSITY:
+    return 3;
+  case VPD_FIELD_STATE:
+    return h ? h->c.nstatev : -1;
+  case VPD_FIELD_DEFGRAD: case VPD_FIELD_STRESS_COROTATIONAL: case VPD_FIELD_STRESS_SPATIAL:
+  case VPD_FIELD_STRAIN: case VPD_FIELD_ROTATION: case VPD_FIELD_LEFT_STRETCH: case VPD_FIELD_SHAPE_INVERSE:
+    return 9;
+  default:
+    return -1;
+  }
+}
+
+int vpd_create(const vpd_case *c, const double *positions, const double *volumes, vpd_handle **out) {
+  if (!out)
+    return set_error(VPD_ERR_INVALID, "out is NULL");
+  *out = nullptr;
+  vpd_handle *h = new vpd_handle();
+  const int rc = create_impl(h, c, positions, volumes);
+  if (rc) {
+    const std::string msg = g_error;
+    destroy_impl(h);
+    g_error = msg;
+    return rc;
+  }
+  *out = h;
+  return VPD_OK;
+}
+
+int vpd_destroy(vpd_handle *h) {
+  if (h)
+    destroy_impl(h);
+  return VPD_OK;
+}
+
+int64_t vpd_num_points(const vpd_handle *h) { return h ? h->n : -1; }
+int64_t vpd_num_bonds(const vpd_handle *h) { return h ? h->nbonds : -1; }
+void *vpd_stream(vpd_handle *h) { return h ? (void *)h->stream : nullptr; }
+int vpd_last_step_ms(const vpd_handle *h, double *ms) {
+  if (!h || !ms)
+    return set_error(VPD_ERR_INVALID, "NULL argument");
+  *ms = h->last_ms;
+  return VPD_OK;
+}
+
+int vpd_step(vpd_handle *h, int32_t nsteps, double *diag_out) {
+  if (!h || nsteps < 0)
+    return set_error(VPD_ERR_INVALID, "vpd_step needs a handle and nsteps >= 0");
+  if (nsteps == 0)
+    return VPD_OK;
+  int rc = ensure_graph(h);
+  if (rc)
+    return rc;
+  VPD_CUDA(cudaEventRecord(h->ev0, h->stream));
+  int64_t done = 0;
+  while (done < nsteps) {
+    const int64_t chunk = std::min<int64_t>(nsteps - done, kDiagRing);
+    int64_t k = 0;
+    for (; k + h->graph_steps <= chunk; k += h->graph_steps)
+      VPD_CUDA(cudaGraphLaunch(h->graph, h->stream));
+    for (; k < chunk; ++k)
+      if ((rc = launch_increment(h->params, h->stream)))
+        return rc;
+    if (diag_out && (rc = copy_rows(h, h->step + done + 1, chunk, diag_out + done * VPD_DIAG_COLS)))
+      return rc;
+    done += chunk;
+    if (done < nsteps && diag_out)
+      VPD_CUDA(cudaStreamSynchronize(h->stream));  // ring slots are reused by the next chunk
+  }
+  VPD_CUDA(cudaEventRecord(h->ev1, h->stream));
+  VPD_CUDA(cudaStreamSynchronize(h->stream));
+  VPD_CUDA(cudaEventElapsedTime(&h->last_ms, h->ev0, h->ev1));
+  h->step += nsteps;
+  return read_status(h);
+}
+
+int vpd_profile_increment(vpd_handle *h, int32_t nsteps, double *stage_ms) {
+  if (!h || !stage_ms || nsteps < 1)
+    return set_error(VPD_ERR_INVALID, "vpd_profile_increment needs a handle, nsteps >= 1 and an output");
+  cudaEvent_t ev[kStages + 1];
+  for (auto &e : ev)
+    VPD_CUDA(cudaEventCreate(&e));
+  for (int k = 0; k < kStages; ++k)
+    stage_ms[k] = 0.0;
+  int rc = VPD_OK;
+  for (int32_t it = 0; it < nsteps && rc == VPD_OK; ++it) {
+    VPD_CUDA(cudaEventRecord(ev[0], h->stream));
+    for (int k = 0; k < kStages && rc == VPD_OK; ++k) {
+      rc = launch_stage(k, h->params, h->stream);
+      VPD_CUDA(cudaEventRecord(ev[k + 1], h->stream));
+    }
+    VPD_CUDA(cudaStreamSynchronize(h->stream));
+    for (int k = 0; k < kStages; ++k) {
+      float ms = 0.0f;
+      VPD_CUDA(cudaEventElapsedTime(&ms, ev[k], ev[k + 1]));
+      stage_ms[k] += ms / nsteps;
+    }
+  }
+  for (auto &e : ev)
+    cudaEventDestroy(e);
+  if (rc)
+    return rc;
+  h->step += nsteps;
+  return read_status(h);
+}
+
+int vpd_neighbors(vpd_handle *h, int64_t *row_ptr, int32_t *col) {
+  if (!h || !row_ptr || !col)
+    return set_error(VPD_ERR_INVALID, "NULL argument");
+  VPD_CUDA(cudaMemcpyAsync(row_ptr, h->row_ptr, sizeof(int64_t) * (h->n + 1), cudaMemcpyDeviceToHost, h->stream));
+  VPD_CUDA(cudaMemcpyAsync(col, h->col, sizeof(int32_t) * h->nbonds, cudaMemcpyDeviceToHost, h->stream));
+  VPD_CUDA(cudaStreamSynchronize(h->stream));
+  return VPD_OK;
+}
+
+int vpd_download(vpd_handle *h, int32_t field, double *out) {
+  if (!h || !out)
+    return set_error(VPD_ERR_INVALID, "NULL argument");
+  const int64_t n = h->n;
+  cudaStream_t s = h->stream;
+  auto get4 = [&](const double4 *src, int comps) -> int {
+    std::vector<double4> buf((size_t)n);
+    VPD_CUDA(cudaMemcpyAsync(buf.data(), src, sizeof(double4) * n, cudaMemcpyDeviceToHost, s));
+    VPD_CUDA(cudaStreamSynchronize(s));
+    for (int64_t i = 0; i < n; ++i) {
+      const double v[4] = {buf[i].x, buf[i].y, buf[i].z, buf[i].w};
+      if (comps == 1)
+        out[i] = v[3];
+      else
+        for (int d = 0; d < 3; ++d)
+          out[3 * i + d] = v[d];
+    }
+    return VPD_OK;
+  };
+  auto getSoA = [&](const double *src, int comps, std::vector<double> &buf) -> int {
+    buf.resize((size_t)(comps * n));
+    VPD_CUDA(cudaMemcpyAsync(buf.data(), src, sizeof(double) * comps * n, cudaMemcpyDeviceToHost, s));
+    VPD_CUDA(cudaStreamSynchronize(s));
+    return VPD_OK;
+  };
+  auto aos = [&](const double *src, int comps) -> int {
+    std::vector<double> buf;
+    int rc = getSoA(src, comps, buf);
+    if (rc)
+      return rc;
+    for (int64_t i = 0; i < n; ++i)
+      for (int c = 0; c < comps; ++c)
+        out[comps * i + c] = buf[c * n + i];
+    return VPD_OK;
+  };
+  auto sym = [&](const double *src) -> int {  // Voigt 11,22,33,23,13,12 -> full 3x3
+    std::vector<double> buf;
+    int rc = getSoA(src, 6, buf);
+    if (rc)
+      return rc;
+    for (int64_t i = 0; i < n; ++i) {
+      const double v[6] = {buf[i], buf[n + i], buf[2 * n + i], buf[3 * n + i], buf[4 * n + i], buf[5 * n + i]};
+      double *o = out + 9 * i;
+      o[0] = v[0], o[1] = v[5], o[2] = v[4], o[3] = v[5], o[4] = v[1], o[5] = v[3];
+      o[6] = v[4], o[7] = v[3], o[8] = v[2];
+    }
+    return VPD_OK;
+  };
+  switch (field) {
+  case VPD_FIELD_POSITION: return get4(h->xv, 3);
+  case VPD_FIELD_VOLUME: return get4(h->xv, 1);
+  case VPD_FIELD_DISPLACEMENT: return get4((h->step & 1) ? h->u1 : h->u0, 3);
+  case VPD_FIELD_VELOCITY: return get4(h->vel, 3);
+  case VPD_FIELD_ACCELERATION: return get4(h->acc, 3);
+  case VPD_FIELD_FORCE_DENSITY: return get4(h->force, 3);
+  case VPD_FIELD_DEFGRAD: return aos(h->Fn, 9);
+  case VPD_FIELD_ROTATION: return aos(h->Rn, 9);
+  case VPD_FIELD_LEFT_STRETCH: return aos(h->Vn, 9);
+  case VPD_FIELD_SHAPE_INVERSE: return aos(h->kinv, 9);
+  case VPD_FIELD_STATE: return aos(h->state, h->c.nstatev);
+  case VPD_FIELD_ENERGY_INTERNAL: return aos(h->eI, 1);
+  case VPD_FIELD_ENERGY_INELASTIC: return aos(h->eP, 1);
+  case VPD_FIELD_STRESS_COROTATIONAL: return sym(h->sig);
+  case VPD_FIELD_STRAIN: return sym(h->En);
+  case VPD_FIELD_STRESS_SPATIAL: {
+    std::vector<double> sg, r;
+    int rc;
+    if ((rc = getSoA(h->sig, 6, sg)) || (rc = getSoA(h->Rn, 9, r)))
+      return rc;
+    for (int64_t i = 0; i < n; ++i) {
+      const double v[6] = {sg[i], sg[n + i], sg[2 * n + i], sg[3 * n + i], sg[4 * n + i], sg[5 * n + i]};
+      const double f[9] = {v[0], v[5], v[4], v[5], v[1], v[3], v[4], v[3], v[2]};
+      double R[9], tmp[9];
+      for (int c = 0; c < 9; ++c)
+        R[c] = r[c * n + i];
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b)
+          tmp[3 * a + b] = f[3 * a] * R[3 * b] + f[3 * a + 1] * R[3 * b + 1] + f[3 * a + 2] * R[3 * b + 2];
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b)
+          out[9 * i + 3 * a + b] = R[3 * a] * tmp[b] + R[3 * a + 1] * tmp[3 + b] + R[3 * a + 2] * tmp[6 + b];
+    }
+    return VPD_OK;
+  }
+  case VPD_FIELD_TEMPERATURE: {
+    std::vector<double> st;
+    int rc = getSoA(h->state, 3, st);
+    if (rc)
+      return rc;
+    for (int64_t i = 0; i < n; ++i)
+      out[i] = st[i] != 0.0 ? st[2 * n + i] : h->c.reference_temperature;
+    return VPD_OK;
+  }
+  case VPD_FIELD_DAMAGE_INDEX: {
+    double *d = nullptr;
+    VPD_CUDA(cudaMalloc(&d, sizeof(double) * n));
+    k_damage_index<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, h->xv, h->len, h->slice_off, h->sell,
+                                                              h->words, d);
+    cudaError_t e = cudaMemcpyAsync(out, d, sizeof(double) * n, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess)
+      e = cudaStreamSynchronize(s);
+    cudaFree(d);
+    if (e != cudaSuccess)
+      return cuda_error(e, "damage index");
+    return VPD_OK;
+  }
+  default:
+    return set_error(VPD_ERR_INVALID, "unknown field");
+  }
+}
+
+}  // extern "C"

@@ -1,0 +1,149 @@
+// Johnson-Cook VUMAT as a device function, one material point per thread.
+//
+// Same update as materials/examples/JohnsonCook.f90:74-156 and the same state layout
+// (init flag, eqps, temperature, yield stress, last plastic increment, cumulative
+// iterations): elastic trial, first-call initialisation, the bracketed bisection return map
+// (at most 50 iterations, warm start from the previous increment, |q - sigma_y| < E 1e-9),
+// radial scaling, energies and adiabatic heating. Stress and strain increments use the
+// legacy_vumat_pd Voigt order 11,22,33,23,13,12 with tensor shear.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <math.h>
+
+namespace vpd {
+
+struct JcParams {
+  double young, poisson, a0, b0, rateC, hardN, thermalM, rate0, tref, tmelt, rho, beta, cp,
+      workToHeat;
+  double mu, lambda, tolerance;
+};
+
+inline JcParams make_jc_params(const double *props) {
+  JcParams p;
+  p.young = props[0], p.poisson = props[1], p.a0 = props[2], p.b0 = props[3];
+  p.rateC = props[4], p.hardN = props[5], p.thermalM = props[6], p.rate0 = props[7];
+  p.tref = props[8], p.tmelt = props[9], p.rho = props[10], p.beta = props[11];
+  p.cp = props[12], p.workToHeat = props[13];
+  p.mu = p.young / (2.0 * (1.0 + p.poisson));
+  p.lambda = p.young * p.poisson / ((1.0 + p.poisson) * (1.0 - 2.0 * p.poisson));
+  p.tolerance = p.young * 1.0e-9;
+  return p;
+}
+
+// Flow stress (JohnsonCook.f90:160-170).
+__device__ __forceinline__ double jc_yield(const JcParams &p, double ep, double rate,
+                                           double temp) {
+  double theta = (temp - p.tref) / (p.tmelt - p.tref);
+  theta = theta > 0.0 ? theta : 0.0;
+  theta = theta < 1.0 ? theta : 1.0;
+  const double effectiveRate = rate == 0.0 ? p.rate0 : rate;
+  return (p.a0 + p.b0 * pow(ep, p.hardN)) * (1.0 - pow(theta, p.thermalM)) *
+         (1.0 + p.rateC * log(effectiveRate / p.rate0));
+}
+
+struct JcPoint {
+  double stress[6];   // in: old corotational stress; out: new
+  double state[6];    // in/out: [init, eqps, T, sigma_y, last deps, sum iterations]
+  double eInternal;   // in/out
+  double eInelastic;  // in/out
+};
+
+// One increment for one point. inc: strain increment (Voigt, tensor shear). Returns the
+// bisection iteration count (0 on the initialising call).
+__device__ __forceinline__ int jc_update(const JcParams &p, double dt, const double *inc,
+                                         JcPoint &pt) {
+  const double traceInc = inc[0] + inc[1] + inc[2];
+  double trial[6];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+    trial[i] = pt.stress[i] + p.lambda * traceInc + 2.0 * p.mu * inc[i];
+#pragma unroll
+  for (int i = 3; i < 6; ++i)
+    trial[i] = pt.stress[i] + 2.0 * p.mu * inc[i];
+
+  if (pt.state[0] == 0.0) {  // first call (:92-102)
+    pt.state[0] = 1.0, pt.state[1] = 0.0, pt.state[2] = p.tref;
+    pt.state[3] = 0.0, pt.state[4] = 0.0, pt.state[5] = 1.0;
+#pragma unroll
+    for (int i = 0; i < 6; ++i)
+      pt.stress[i] = trial[i];
+    return 0;
+  }
+  const double epOld = pt.state[1], temperature = pt.state[2], oldYield = pt.state[3];
+  const double pressure = (trial[0] + trial[1] + trial[2]) / 3.0;
+  double dev[6];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+    dev[i] = trial[i] - pressure;
+#pragma unroll
+  for (int i = 3; i < 6; ++i)
+    dev[i] = trial[i];
+  const double qTrial =
+      sqrt(1.5 * (dev[0] * dev[0] + dev[1] * dev[1] + dev[2] * dev[2] +
+                  2.0 * (dev[3] * dev[3] + dev[4] * dev[4] + dev[5] * dev[5])));
+
+  // Bracketed bisection with warm start (:114-136).
+  double epInc = 0.0, epLower = 0.0, epUpper = qTrial / (2.0 * p.mu), yield = oldYield;
+  int iteration = 0;
+  while (iteration < 50) {
+    ++iteration;
+    const double epRate = epInc / dt;
+    yield = jc_yield(p, epOld + epInc, epRate, temperature);
+    yield = yield > oldYield ? yield : oldYield;
+    double qNew = qTrial - 3.0 * p.mu * epInc;
+    qNew = qNew > 0.0 ? qNew : 0.0;
+    const double residual = qNew - yield;
+    if (fabs(residual) < p.tolerance)
+      break;
+    if (epInc == 0.0 && residual < 0.0)
+      break;
+    if (residual >= 0.0)
+      epLower = epLower > epInc ? epLower : epInc;
+    else
+      epUpper = epUpper < epInc ? epUpper : epInc;
+    epInc = 0.5 * (epLower + epUpper);
+    if (iteration == 1) {
+      double warm = pt.state[4];
+      warm = warm > epLower ? warm : epLower;
+      epInc = warm < epUpper ? warm : epUpper;
+    }
+  }
+
+  double updated[6];
+#pragma unroll
+  for (int i = 0; i < 6; ++i)
+    updated[i] = trial[i];
+  if (qTrial > 0.0) {  // radial scaling (:138-142)
+    double scale = 1.0 - 3.0 * p.mu * epInc / qTrial;
+    scale = scale > 0.0 ? scale : 0.0;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+      updated[i] = pressure + scale * dev[i];
+#pragma unroll
+    for (int i = 3; i < 6; ++i)
+      updated[i] = scale * dev[i];
+  }
+  double qNew = qTrial - 3.0 * p.mu * epInc;
+  qNew = qNew > 0.0 ? qNew : 0.0;
+  double work = 0.0;
+#pragma unroll
+  for (int i = 0; i < 6; ++i)
+    work += (pt.stress[i] + updated[i]) * inc[i];
+  const double workInc = 0.5 * work;
+  const double plasticWork = 0.5 * epInc * qNew;
+#pragma unroll
+  for (int i = 0; i < 6; ++i)
+    pt.stress[i] = updated[i];
+  pt.eInternal += workInc / p.rho;
+  pt.eInelastic += plasticWork / p.rho;
+  pt.state[0] = 1.0;
+  pt.state[1] = epOld + epInc;
+  pt.state[2] = temperature + p.workToHeat * p.beta * plasticWork / (p.rho * p.cp);
+  pt.state[3] = yield;
+  pt.state[4] = epInc;
+  pt.state[5] = pt.state[5] + (double)iteration;
+  return iteration;
+}
+
+}  // namespace vpd
