@@ -206,6 +206,18 @@ int vpd_force_density(const double *positions, const double *volumes, int64_t n,
                       const int64_t *row_ptr, const int32_t *col, const double *kinv,
                       const double *defgrad, const double *cauchy_stress,
                       const double *bond_damage, double *force, void *stream);
+/* vpd_force_density without any device allocation, for hosts that cannot allocate device
+   memory during a step (all device memory handed to their own pool, or a step loop that
+   cannot take the device-wide synchronisation of cudaMalloc/cudaFree). Same arguments,
+   results and errors as vpd_force_density; its scratch is a fixed array inside the library
+   (about 4.7 MB held on each GPU that loads it). At most 65536 points per call, else
+   VPD_ERR_CAPACITY. Calls share the scratch: calls that overlap on the GPU race. The first
+   call on a device looks up the scratch address; make it before any stream capture.
+   Synchronises the stream. (No counterpart in the reference.) */
+int vpd_force_density_noalloc(const double *positions, const double *volumes, int64_t n,
+                              const int64_t *row_ptr, const int32_t *col, const double *kinv,
+                              const double *defgrad, const double *cauchy_stress,
+                              const double *bond_damage, double *force, void *stream);
 /* Per point: F_n, F_n+1, V_n, R_n -> D-bar (unrotated rate of deformation), relative spin
    increment, R_n+1, V_n+1, Green-Lagrange E(F_n+1); all [9] per point. */
 int vpd_corotational_update(int64_t n, const double *defgrad_old, const double *defgrad_new,

@@ -80,6 +80,8 @@ def library():
     lib.vpd_shape_tensor_inverse.argtypes = [_VP, _VP, ctypes.c_int64, _VP, _VP, _VP, _VP]
     lib.vpd_deformation_gradients.argtypes = [_VP, _VP, _VP, ctypes.c_int64, _VP, _VP, _VP, _VP, _VP]
     lib.vpd_force_density.argtypes = [_VP, _VP, ctypes.c_int64, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP]
+    lib.vpd_force_density_noalloc.argtypes = [_VP, _VP, ctypes.c_int64, _VP, _VP, _VP, _VP, _VP,
+                                              _VP, _VP, _VP]
     lib.vpd_corotational_update.argtypes = [ctypes.c_int64, _VP, _VP, _VP, _VP, ctypes.c_double,
                                             _VP, _VP, _VP, _VP, _VP, _VP]
     lib.vpd_material_update.argtypes = [ctypes.c_int64, _D, ctypes.c_int32, ctypes.c_double] + [_VP] * 12
@@ -224,6 +226,18 @@ def force_density(positions, volumes, row_ptr, col, kinv, defgrad, stress, bond_
     _check(library().vpd_force_density(_ptr(positions), _ptr(volumes), positions.shape[0],
                                        _ptr(row_ptr), _ptr(col), _ptr(kinv), _ptr(defgrad),
                                        _ptr(stress), _ptr(bond_damage), _ptr(out), _stream()))
+    return out
+
+
+def force_density_noalloc(positions, volumes, row_ptr, col, kinv, defgrad, stress, out,
+                          bond_damage=None):
+    """force_density for callers that cannot allocate device memory: the library allocates
+    nothing (its scratch is a fixed array, at most 65536 points per call) and writes into the
+    caller's ``out`` [n,3]. Calls that overlap on the GPU share that scratch and race."""
+    _check(library().vpd_force_density_noalloc(_ptr(positions), _ptr(volumes), positions.shape[0],
+                                               _ptr(row_ptr), _ptr(col), _ptr(kinv),
+                                               _ptr(defgrad), _ptr(stress), _ptr(bond_damage),
+                                               _ptr(out), _stream()))
     return out
 
 
