@@ -170,6 +170,9 @@ int vpd_create(const vpd_case *c, const double *positions, const double *volumes
 int vpd_destroy(vpd_handle *h);
 int64_t vpd_num_points(const vpd_handle *h);
 int64_t vpd_num_bonds(const vpd_handle *h);
+/* Bond layout the kernels stream: the number of 32-slot lattice-stencil bit-mask words per
+   point, or 0 for the sliced-ELL index layout. (No reference counterpart.) */
+int vpd_bond_layout_words(const vpd_handle *h);
 /* Advances nsteps increments. diag_out (host, may be NULL) receives nsteps rows of
    VPD_DIAG_COLS doubles. Returns after the increments completed on the device. */
 int vpd_step(vpd_handle *h, int32_t nsteps, double *diag_out);
@@ -182,8 +185,9 @@ int vpd_neighbors(vpd_handle *h, int64_t *row_ptr, int32_t *col);
 void *vpd_stream(vpd_handle *h);
 int vpd_last_step_ms(const vpd_handle *h, double *ms);
 /* Advances nsteps increments launching each kernel separately, with CUDA events between
-   them on the handle's stream; stage_ms[3] receives the mean device time of the
-   deformation, material and force kernels. Diagnostics rows are kept on the device only.
+   them on the handle's stream; stage_ms[4] receives the mean device time of the
+   deformation, material, force and integration kernels. Diagnostics rows are kept on the
+   device only.
    (No reference counterpart: per-stage timing of the step loop.) */
 int vpd_profile_increment(vpd_handle *h, int32_t nsteps, double *stage_ms);
 
@@ -239,6 +243,21 @@ int vpd_damage_update(const double *positions, const double *displacement,
                       const double *volumes, int64_t n, const int64_t *row_ptr,
                       const int32_t *col, double initiation, double failure,
                       double *bond_damage, double *damage_index, void *stream);
+
+/* ---- surrogate network (no reference counterpart: the learned Johnson-Cook update) ----
+   10 -> 128 -> 128 -> 128 -> 7, SiLU, BF16 weights, FP32 accumulation on the tensor cores.
+   Parameters: `weights` are VPD_MLP_WEIGHTS bf16 values (uint16 bit patterns), w1 [128][16],
+   w2 [128][128], w3 [128][128], w4 [16][128] row-major [out][in]; `biases` are b1 [128],
+   b2 [128], b3 [128], b4 [16] floats. Inputs and outputs are padded to 16 columns. */
+#define VPD_MLP_WEIGHTS 36864
+#define VPD_MLP_PARAMS 37264
+/* out [batch][16] = network(x [batch][16]). Synchronises the stream. */
+int vpd_mlp_forward(const uint16_t *weights, const float *biases, const float *x, int64_t batch,
+                    float *out, void *stream);
+/* grad [VPD_MLP_PARAMS] (weights then biases, FP32) = d/dparams of sum(out * gout), i.e. the
+   backward pass for the output gradient gout [batch][16]. Synchronises the stream. */
+int vpd_mlp_gradients(const uint16_t *weights, const float *biases, const float *x,
+                      const float *gout, int64_t batch, float *grad, void *stream);
 
 /* Plugin ABI: the Johnson-Cook VUMAT evaluated on the GPU for one block of host arrays
    in the reference's column-major [component][nblock] layout. Synchronous. A failure is

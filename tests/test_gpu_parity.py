@@ -196,6 +196,21 @@ def test_increment_matches_oracle_full_tensile_bar_1():
     assert nrmse(fields["stress_spatial"], o.get("stress_spatial")) < 1e-6
 
 
+def test_sliced_ell_layout_matches_stencil_layout(monkeypatch):
+    """The sliced-ELL bond layout (used when points do not form the lattice in index order)
+    gives the same increments as the lattice-stencil layout."""
+    case = tensile_bar(1, jitter=0.05, jitter_seed=7, damage_mode=1, damage_initiation=0.004)
+    with vpd.Simulation(case) as a:
+        ra = a.step(200)
+        ua, da = a.field("displacement"), a.field("damage_index")
+    monkeypatch.setenv("VPD_BOND_LAYOUT", "ell")
+    with vpd.Simulation(case) as b:
+        rb = b.step(200)
+        assert nrmse(rb[:, STRESS], ra[:, STRESS]) < 1e-9
+        assert max_rel(b.field("displacement"), ua) < 1e-9
+        assert np.array_equal(b.field("damage_index"), da)
+
+
 def test_graph_and_stage_launches_agree_bitwise():
     case = tensile_bar(1, jitter=0.05, jitter_seed=9, damage_mode=1, damage_initiation=0.003)
     with vpd.Simulation(case) as a, vpd.Simulation(case) as b:

@@ -225,7 +225,8 @@ struct vpd_handle {
   int32_t *col = nullptr, *len = nullptr, *sell = nullptr;
   uint32_t *words = nullptr;
   double *kinv = nullptr, *F = nullptr, *Fn = nullptr, *Vn = nullptr, *Rn = nullptr, *En = nullptr;
-  double *sig = nullptr, *state = nullptr, *eI = nullptr, *eP = nullptr, *M = nullptr, *obsw = nullptr;
+  double *sig = nullptr, *state = nullptr, *eI = nullptr, *eP = nullptr, *Mt = nullptr, *obsw = nullptr;
+  StencilLayout st;
   double *part_mat = nullptr, *part_force = nullptr, *accum = nullptr, *diag = nullptr;
   uint8_t *flags = nullptr;
   unsigned *status_dev = nullptr, *counter = nullptr;
@@ -270,8 +271,8 @@ int check_case(const vpd_case *c) {
     return set_error(VPD_ERR_INVALID, "critical_stretch requires initiation > 0.");
   if (c->damage_mode != VPD_DAMAGE_NONE && c->damage_mode != VPD_DAMAGE_CRITICAL_STRETCH)
     return set_error(VPD_ERR_INVALID, "unknown damage mode");
-  if (c->precision != VPD_PRECISION_FP64)
-    return set_error(VPD_ERR_UNSUPPORTED, "this build implements the FP64 precision mode only");
+  if (c->precision != VPD_PRECISION_FP64 && c->precision != VPD_PRECISION_MIXED)
+    return set_error(VPD_ERR_INVALID, "unknown precision mode");
   if (c->material_mode != VPD_MATERIAL_VUMAT)
     return set_error(VPD_ERR_UNSUPPORTED, "this build implements the plain VUMAT material only");
   for (int k = 0; k < 14; ++k)
@@ -336,7 +337,7 @@ int create_impl(vpd_handle *h, const vpd_case *c, const double *positions, const
       (rc = dalloc(h, &h->Fn, 9 * n)) || (rc = dalloc(h, &h->Vn, 9 * n)) ||
       (rc = dalloc(h, &h->Rn, 9 * n)) || (rc = dalloc(h, &h->En, 6 * n)) ||
       (rc = dalloc(h, &h->sig, 6 * n)) || (rc = dalloc(h, &h->state, (size_t)c->nstatev * n)) ||
-      (rc = dalloc(h, &h->eI, n)) || (rc = dalloc(h, &h->eP, n)) || (rc = dalloc(h, &h->M, 9 * n)) ||
+      (rc = dalloc(h, &h->eI, n)) || (rc = dalloc(h, &h->eP, n)) || (rc = dalloc(h, &h->Mt, 10 * n)) ||
       (rc = dalloc(h, &h->obsw, n)) || (rc = dalloc(h, &h->flags, n)) ||
       (rc = dalloc(h, &h->row_ptr, n + 1)) || (rc = dalloc(h, &h->step_dev, 1)) ||
       (rc = dalloc(h, &h->status_dev, 1)) || (rc = dalloc(h, &h->counter, 1)) ||
@@ -381,16 +382,25 @@ int create_impl(vpd_handle *h, const vpd_case *c, const double *positions, const
     if (rc)
       return rc;
   }
-  if ((rc = build_sell(h->row_ptr, h->col, n, &h->len, &h->slice_off, &h->sell, &h->sell_total, s)))
+  // the bond layout the kernels stream: lattice-stencil bit masks when the points form the
+  // lattice in index order (every generated patch), else the sliced ELL
+  // (VPD_BOND_LAYOUT=ell selects the sliced ELL for any case)
+  const char *layout = getenv("VPD_BOND_LAYOUT");
+  if (!(layout && std::string(layout) == "ell") &&
+      (rc = build_stencil(h->row_ptr, h->col, n, c->ny, c->nz, c->spacing, h->st, s)))
     return rc;
-  h->allocations.push_back(h->len);
-  h->allocations.push_back(h->slice_off);
-  h->allocations.push_back(h->sell);
-  if ((rc = dalloc(h, &h->words, (size_t)(h->sell_total / 32))))
-    return rc;
-  VPD_CUDA(cudaMemsetAsync(h->words, 0, sizeof(uint32_t) * std::max<int64_t>(h->sell_total / 32, 1), s));
+  if (h->st.nw == 0) {
+    if ((rc = build_sell(h->row_ptr, h->col, n, &h->len, &h->slice_off, &h->sell, &h->sell_total, s)))
+      return rc;
+    h->allocations.push_back(h->len);
+    h->allocations.push_back(h->slice_off);
+    h->allocations.push_back(h->sell);
+    if ((rc = dalloc(h, &h->words, (size_t)(h->sell_total / 32))))
+      return rc;
+    VPD_CUDA(cudaMemsetAsync(h->words, 0, sizeof(uint32_t) * std::max<int64_t>(h->sell_total / 32, 1), s));
+  }
   const int mat_blocks = material_grid(n);
-  const int force_blocks = (int)(((n + 31) / 32 * 32 + kBondThreads - 1) / kBondThreads);
+  const int force_blocks = integrate_grid(n);
   if ((rc = dalloc(h, &h->part_mat, (size_t)mat_blocks * PM_COUNT)) ||
       (rc = dalloc(h, &h->part_force, (size_t)force_blocks * PF_COUNT)))
     return rc;
@@ -403,7 +413,8 @@ int create_impl(vpd_handle *h, const vpd_case *c, const double *positions, const
   p.xv = h->xv, p.len = h->len, p.slice_off = h->slice_off, p.sell = h->sell, p.words = h->words;
   p.u0 = h->u0, p.u1 = h->u1, p.vel = h->vel, p.acc = h->acc, p.force = h->force;
   p.kinv = h->kinv, p.F = h->F, p.Fn = h->Fn, p.Vn = h->Vn, p.Rn = h->Rn, p.En = h->En;
-  p.sig = h->sig, p.state = h->state, p.eI = h->eI, p.eP = h->eP, p.M = h->M;
+  p.sig = h->sig, p.state = h->state, p.eI = h->eI, p.eP = h->eP, p.Mt = h->Mt;
+  p.st = h->st;
   p.nstatev = c->nstatev;
   p.flags = h->flags, p.obsw = h->obsw;
   p.jc = make_jc_params(c->props);
@@ -415,6 +426,18 @@ int create_impl(vpd_handle *h, const vpd_case *c, const double *positions, const
   p.use_compression = c->damage_failure > 0.0 && std::isfinite(c->damage_failure);
   p.tension2 = (1.0 + c->damage_initiation) * (1.0 + c->damage_initiation);
   p.compression2 = c->damage_failure < 1.0 ? (1.0 - c->damage_failure) * (1.0 - c->damage_failure) : 0.0;
+  p.tension2f = (float)p.tension2, p.compression2f = (float)p.compression2;
+  if (c->precision == VPD_PRECISION_MIXED) {
+    if (!h->st.nw)
+      return set_error(VPD_ERR_UNSUPPORTED,
+                       "mixed precision needs the points in lattice order (lattice-stencil bonds)");
+    float4 *jit = nullptr;
+    if ((rc = dalloc(h, &jit, n)) || (rc = dalloc(h, &p.uf, n)) || (rc = dalloc(h, &p.Gf, 9 * n)) ||
+        (rc = dalloc(h, &p.Mf, 12 * n)))
+      return rc;
+    p.jit = jit;
+    p.mixed = 1;
+  }
   p.step = h->step_dev, p.status = h->status_dev;
   p.part_mat = h->part_mat, p.part_force = h->part_force, p.accum = h->accum, p.diag = h->diag;
   p.counter = h->counter;
@@ -423,9 +446,11 @@ int create_impl(vpd_handle *h, const vpd_case *c, const double *positions, const
   p.area = sets.area, p.n_lat_pos = sets.n_lat_pos, p.n_lat_neg = sets.n_lat_neg;
   p.sign = (c->bc_mode == VPD_BC_SMOOTH_DISPLACEMENT ? c->amplitude : c->grip_velocity) > 0.0 ? 1.0 : -1.0;
 
-  if ((rc = launch_shape_inverse_sell(p, s)))
+  if ((rc = p.st.nw ? launch_shape_stencil(p, s) : launch_shape_inverse_sell(p, s)))
     return rc;
   if ((rc = launch_init(p, s)))
+    return rc;
+  if (p.mixed && (rc = launch_mixed_setup(p, c->ny, c->nz, hsp, yoff, zoff, s)))
     return rc;
   const double acc0[ACC_COUNT] = {0.0, 0.0, 0.0, 1.0};
   const int64_t one = 1;
@@ -441,6 +466,7 @@ void destroy_impl(vpd_handle *h) {
     cudaStreamSynchronize(h->stream);
   for (void *p : h->allocations)
     cudaFree(p);
+  free_stencil(h->st);
   if (h->ev0)
     cudaEventDestroy(h->ev0);
   if (h->ev1)
@@ -540,6 +566,7 @@ int vpd_destroy(vpd_handle *h) {
 
 int64_t vpd_num_points(const vpd_handle *h) { return h ? h->n : -1; }
 int64_t vpd_num_bonds(const vpd_handle *h) { return h ? h->nbonds : -1; }
+int vpd_bond_layout_words(const vpd_handle *h) { return h ? h->st.nw : -1; }
 void *vpd_stream(vpd_handle *h) { return h ? (void *)h->stream : nullptr; }
 int vpd_last_step_ms(const vpd_handle *h, double *ms) {
   if (!h || !ms)
@@ -714,8 +741,16 @@ int vpd_download(vpd_handle *h, int32_t field, double *out) {
   case VPD_FIELD_DAMAGE_INDEX: {
     double *d = nullptr;
     VPD_CUDA(cudaMalloc(&d, sizeof(double) * n));
-    k_damage_index<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, h->xv, h->len, h->slice_off, h->sell,
-                                                              h->words, d);
+    if (h->st.nw) {
+      const int rc = launch_damage_index_stencil(h->params, d, s);
+      if (rc) {
+        cudaFree(d);
+        return rc;
+      }
+    } else {
+      k_damage_index<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, h->xv, h->len, h->slice_off, h->sell,
+                                                                h->words, d);
+    }
     cudaError_t e = cudaMemcpyAsync(out, d, sizeof(double) * n, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess)
       e = cudaStreamSynchronize(s);

@@ -1,0 +1,215 @@
+// Mixed-precision bond kernels (VPD_PRECISION_MIXED), lattice-stencil layout only.
+//
+// The bond sums run in FP32 on FP32 copies of the data they gather:
+//   jit[i] = (X_i - lattice_i, V_i) as float4, so a bond vector is
+//            xi = (o h) + (jit_j - jit_i) with the slot's lattice offset o h (float, per slot);
+//   uf[i]  = the predicted displacement as float4, written by the integrator;
+//   Mf[i]  = V_i M_i (force map scaled by volume) as 12 floats (three float4).
+// Each 32-slot word is summed in plain FP32 and the word sums are added with Kahan
+// compensation, so the result carries ~1 FP32 ulp of error (relative ~6e-8) rather than the
+// bond count times it. FP64 stays where the update integrates: K^-1, F = I + G K^-1, the
+// polar/rotation update, the Johnson-Cook return map and the integrator (k_material,
+// k_integrate). The critical-stretch test runs in FP32 with a 1e-5 relative margin and falls
+// back to the reference's exact FP64 arithmetic inside the margin, so bond breaking decides
+// exactly as the FP64 path would on the same displacements.
+#include "vpd_math.cuh"
+#include "vpd_step.cuh"
+
+namespace vpd {
+
+__device__ __forceinline__ float4 ldgf4(const float4 *p) { return __ldg(p); }
+
+__device__ __forceinline__ int64_t clamp_index(int64_t j, int64_t n) {
+  return j < 0 ? 0 : (j >= n ? n - 1 : j);
+}
+
+__device__ __forceinline__ void kahan_add(float &s, float &c, float x) {
+  const float y = x - c;
+  const float t = s + y;
+  c = (t - s) - y;
+  s = t;
+}
+
+__device__ __noinline__ bool exact_break_mixed(const double4 *xv, const double4 *U, int64_t i,
+                                               int64_t j, double initiation, double failure,
+                                               int use_compression) {
+  const double4 xi = xv[i], xj = xv[j], ui = U[i], uj = U[j];
+  const double yi0 = __dadd_rn(xi.x, ui.x), yi1 = __dadd_rn(xi.y, ui.y), yi2 = __dadd_rn(xi.z, ui.z);
+  const double y0 = __dsub_rn(__dadd_rn(xj.x, uj.x), yi0);
+  const double y1 = __dsub_rn(__dadd_rn(xj.y, uj.y), yi1);
+  const double y2 = __dsub_rn(__dadd_rn(xj.z, uj.z), yi2);
+  const double e0 = __dsub_rn(xj.x, xi.x), e1 = __dsub_rn(xj.y, xi.y), e2 = __dsub_rn(xj.z, xi.z);
+  const double initial =
+      __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(e0, e0), __dmul_rn(e1, e1)), __dmul_rn(e2, e2)));
+  const double cur =
+      __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(y0, y0), __dmul_rn(y1, y1)), __dmul_rn(y2, y2)));
+  const double stretch = __ddiv_rn(__dsub_rn(cur, initial), initial);
+  return stretch > initiation || (use_compression && stretch < -failure);
+}
+
+// G = sum_j V_j (u_j - u_i) (x) xi in FP32 (written as 9 floats, structure of arrays); the
+// material kernel forms F = I + G K^-1 in FP64.
+template <bool DAMAGE>
+__global__ void __launch_bounds__(kBondThreads, 3) k_deformation_mixed(StepParams p) {
+  const int64_t n = p.n;
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool valid = i < n;
+  const int64_t ii = valid ? i : n - 1;
+  const float4 ji = ldgf4(p.jit + ii), ui = ldgf4(p.uf + ii);
+  float Gs[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, Gc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  const float lo = 1.0f - 1.0e-5f, hi = 1.0f + 1.0e-5f;
+  for (int w = 0; w < p.st.nw; ++w) {
+    const uint32_t m = valid ? __ldg(p.st.mask + (int64_t)w * n + i) : 0u;
+    if (__all_sync(0xffffffffu, m == 0u))
+      continue;
+    const int32_t *dl = p.st.delta + 32 * w;
+    const float4 *ol = p.st.e0 + 32 * w;
+    uint32_t live = 0u, fresh = 0u, near = 0u;
+    if (DAMAGE)
+      live = m & __ldg(p.st.forward + w) & ~p.st.broken[(int64_t)w * n + ii];
+    float G[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll 4
+    for (int b = 0; b < 32; ++b) {
+      const int64_t j = clamp_index(ii + __ldg(dl + b), n);  // contiguous across the warp
+      const float4 o = __ldg(ol + b);
+      const float4 jj = ldgf4(p.jit + j), uj = ldgf4(p.uf + j);
+      const float e0 = o.x + (jj.x - ji.x), e1 = o.y + (jj.y - ji.y), e2 = o.z + (jj.z - ji.z);
+      const float d0 = uj.x - ui.x, d1 = uj.y - ui.y, d2 = uj.z - ui.z;
+      const float v = ((m >> b) & 1u) ? jj.w : 0.0f;  // lanes without this bond add nothing
+      const float w0 = v * d0, w1 = v * d1, w2 = v * d2;
+      G[0] += w0 * e0, G[1] += w0 * e1, G[2] += w0 * e2;
+      G[3] += w1 * e0, G[4] += w1 * e1, G[5] += w1 * e2;
+      G[6] += w2 * e0, G[7] += w2 * e1, G[8] += w2 * e2;
+      if (DAMAGE && ((live >> b) & 1u)) {
+        const float y0 = e0 + d0, y1 = e1 + d1, y2 = e2 + d2;
+        const float yy = y0 * y0 + y1 * y1 + y2 * y2;
+        const float xx = e0 * e0 + e1 * e1 + e2 * e2;
+        const float t = p.tension2f * xx;
+        if (yy > t * hi)
+          fresh |= 1u << b;
+        else if (yy >= t * lo)
+          near |= 1u << b;
+        else if (p.use_compression) {
+          const float c = p.compression2f * xx;
+          if (yy < c * lo)
+            fresh |= 1u << b;
+          else if (yy <= c * hi)
+            near |= 1u << b;
+        }
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < 9; ++c)
+      kahan_add(Gs[c], Gc[c], G[c]);
+    if (DAMAGE && near) {
+      const int64_t step = *p.step;
+      const double4 *U = (step & 1) ? p.u1 : p.u0;
+      for (uint32_t f = near; f; f &= f - 1) {
+        const int b = __ffs(f) - 1;
+        if (exact_break_mixed(p.xv, U, i, i + dl[b], p.dmg_initiation, p.dmg_failure,
+                              p.use_compression))
+          fresh |= 1u << b;
+      }
+    }
+    if (DAMAGE && fresh) {
+      atomicOr(p.st.broken + (int64_t)w * n + i, fresh);
+      for (uint32_t f = fresh; f; f &= f - 1) {
+        const int b = __ffs(f) - 1;
+        const int r = p.st.reverse[32 * w + b];
+        atomicOr(p.st.broken + (int64_t)(r >> 5) * n + (i + dl[b]), 1u << (r & 31));
+      }
+    }
+  }
+  if (!valid)
+    return;
+#pragma unroll
+  for (int c = 0; c < 9; ++c)
+    p.Gf[c * n + i] = Gs[c];
+}
+
+// f = M_i sum V_j xi + sum (V_j M_j) xi over intact bonds, in FP32 with Kahan-folded words.
+__global__ void __launch_bounds__(kBondThreads, 3) k_force_mixed(StepParams p) {
+  const int64_t n = p.n;
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool valid = i < n;
+  const int64_t ii = valid ? i : n - 1;
+  const float4 ji = ldgf4(p.jit + ii);
+  float fs[3] = {0, 0, 0}, fc[3] = {0, 0, 0}, ss[3] = {0, 0, 0}, sc[3] = {0, 0, 0};
+  for (int w = 0; w < p.st.nw; ++w) {
+    uint32_t m = valid ? __ldg(p.st.mask + (int64_t)w * n + i) : 0u;
+    if (p.damage)
+      m &= ~p.st.broken[(int64_t)w * n + ii];
+    if (__all_sync(0xffffffffu, m == 0u))
+      continue;
+    const int32_t *dl = p.st.delta + 32 * w;
+    const float4 *ol = p.st.e0 + 32 * w;
+    float f0 = 0, f1 = 0, f2 = 0, s0 = 0, s1 = 0, s2 = 0;
+#pragma unroll 4
+    for (int b = 0; b < 32; ++b) {
+      const bool bond = (m >> b) & 1u;
+      const int64_t j = clamp_index(ii + __ldg(dl + b), n);  // contiguous across the warp
+      const float4 o = __ldg(ol + b);
+      const float4 jj = ldgf4(p.jit + j);
+      const float e0 = bond ? o.x + (jj.x - ji.x) : 0.0f;
+      const float e1 = bond ? o.y + (jj.y - ji.y) : 0.0f;
+      const float e2 = bond ? o.z + (jj.z - ji.z) : 0.0f;
+      s0 += jj.w * e0, s1 += jj.w * e1, s2 += jj.w * e2;
+      const float4 *Mj = reinterpret_cast<const float4 *>(p.Mf + 12 * j);
+      const float4 a = __ldg(Mj), c = __ldg(Mj + 1), d = __ldg(Mj + 2);
+      f0 += a.x * e0 + a.y * e1 + a.z * e2;
+      f1 += a.w * e0 + c.x * e1 + c.y * e2;
+      f2 += c.z * e0 + c.w * e1 + d.x * e2;
+    }
+    kahan_add(fs[0], fc[0], f0), kahan_add(fs[1], fc[1], f1), kahan_add(fs[2], fc[2], f2);
+    kahan_add(ss[0], sc[0], s0), kahan_add(ss[1], sc[1], s1), kahan_add(ss[2], sc[2], s2);
+  }
+  if (!valid)
+    return;
+  const float4 *Mi4 = reinterpret_cast<const float4 *>(p.Mf + 12 * i);
+  const float4 a = Mi4[0], c = Mi4[1], d = Mi4[2];
+  const double rv = 1.0 / (double)ji.w;
+  const double s0 = ss[0], s1 = ss[1], s2 = ss[2];
+  const double f0 = (double)fs[0] + (a.x * s0 + a.y * s1 + a.z * s2) * rv;
+  const double f1 = (double)fs[1] + (a.w * s0 + c.x * s1 + c.y * s2) * rv;
+  const double f2 = (double)fs[2] + (c.z * s0 + c.w * s1 + d.x * s2) * rv;
+  p.force[i] = make_double4(f0, f1, f2, 0.0);
+}
+
+// FP32 copies for the mixed kernels: jit = (X - lattice position, V), uf = u[1] (the first
+// predicted displacement).
+__global__ void k_mixed_setup(StepParams p, int ny, int nz, double h, double yoff, double zoff) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= p.n)
+    return;
+  const int iz = (int)(i % nz), iy = (int)((i / nz) % ny), ix = (int)(i / ((int64_t)ny * nz));
+  const double4 x = p.xv[i];
+  p.jit[i] = make_float4((float)(x.x - (double)ix * h), (float)(x.y - ((double)iy * h - yoff)),
+                         (float)(x.z - ((double)iz * h - zoff)), (float)x.w);
+  const double4 u = p.u1[i];
+  p.uf[i] = make_float4((float)u.x, (float)u.y, (float)u.z, 0.0f);
+}
+
+int launch_deformation_mixed(const StepParams &p, cudaStream_t s) {
+  const unsigned blocks = (unsigned)((p.n + kBondThreads - 1) / kBondThreads);
+  if (p.damage)
+    k_deformation_mixed<true><<<blocks, kBondThreads, 0, s>>>(p);
+  else
+    k_deformation_mixed<false><<<blocks, kBondThreads, 0, s>>>(p);
+  VPD_CUDA(cudaGetLastError());
+  return VPD_OK;
+}
+
+int launch_force_mixed(const StepParams &p, cudaStream_t s) {
+  k_force_mixed<<<(unsigned)((p.n + kBondThreads - 1) / kBondThreads), kBondThreads, 0, s>>>(p);
+  VPD_CUDA(cudaGetLastError());
+  return VPD_OK;
+}
+
+int launch_mixed_setup(const StepParams &p, int ny, int nz, double h, double yoff, double zoff,
+                       cudaStream_t s) {
+  k_mixed_setup<<<(unsigned)((p.n + 255) / 256), 256, 0, s>>>(p, ny, nz, h, yoff, zoff);
+  VPD_CUDA(cudaGetLastError());
+  return VPD_OK;
+}
+
+}  // namespace vpd

@@ -6,17 +6,17 @@
 //   k_material     corotational kinematics, the Johnson-Cook VUMAT, rotation to the spatial
 //                  frame and the force map M = J sigma F^-T K^-1
 //                  (VumatPdCorrespondenceMaterial::update :72-176, cauchyToFirstPiola :83-91)
-//   k_force        f_i = sum_j (1 - d_ij) (M_i + M_j) xi_ij V_j, velocity-Verlet correction,
-//                  boundary conditions at t_n, diagnostics, then the next increment's
-//                  displacement prediction with boundary conditions at t_n+1
-//                  (computeForceDensity :199-230, ExplicitTimeIntegrator.cpp:23-52,
-//                   BoundaryConditions.cpp:81-115, BoundaryValueCaseRunner.cpp:231-306)
+//   k_force        f_i = sum_j (1 - d_ij) (M_i + M_j) xi_ij V_j (computeForceDensity :199-230)
+//   k_integrate    velocity-Verlet correction, boundary conditions at t_n, diagnostics, then
+//                  the next increment's displacement prediction with boundary conditions at
+//                  t_n+1 (ExplicitTimeIntegrator.cpp:23-52, BoundaryConditions.cpp:81-115,
+//                  BoundaryValueCaseRunner.cpp:231-306)
 //
 // One thread per point; the 32 points of a warp form one sliced-ELL slice, so the neighbour
 // index loads are coalesced and the bond loop runs to the slice width with the tail masked.
 // The increment number lives in device memory (*step), so the launch sequence is
 // independent of the host and can be captured in a CUDA graph. Diagnostics are reduced
-// deterministically: each block writes a partial, the last block of k_force sums them in
+// deterministically: each block writes a partial, the last block of k_integrate sums them in
 // block order and writes the increment's row.
 #include "vpd_math.cuh"
 #include "vpd_step.cuh"
@@ -204,9 +204,22 @@ __global__ void __launch_bounds__(kMaterialThreads) k_material(StepParams p) {
   double maxEqps = 0.0;
   if (i < n) {
     double F[9], Fn[9], Vn[9], Rn[9];
+    if (p.mixed) {  // F = I + G K^-1 in FP64 from the FP32 bond sum
+      double G[9], K[9];
+#pragma unroll
+      for (int c = 0; c < 9; ++c)
+        G[c] = (double)p.Gf[c * n + i], K[c] = p.kinv[c * n + i];
+      m_mul(G, K, F);
+#pragma unroll
+      for (int c = 0; c < 9; c += 4)
+        F[c] += 1.0;
+    } else {
+#pragma unroll
+      for (int c = 0; c < 9; ++c)
+        F[c] = p.F[c * n + i];
+    }
 #pragma unroll
     for (int c = 0; c < 9; ++c) {
-      F[c] = p.F[c * n + i];
       Fn[c] = p.Fn[c * n + i];
       Vn[c] = p.Vn[c * n + i];
       Rn[c] = p.Rn[c * n + i];
@@ -252,7 +265,23 @@ __global__ void __launch_bounds__(kMaterialThreads) k_material(StepParams p) {
       p.Fn[c * n + i] = F[c];
       p.Vn[c * n + i] = co.v[c];
       p.Rn[c * n + i] = co.r[c];
-      p.M[c * n + i] = M[c];
+    }
+    // the force map scaled by the point's volume, 10 doubles per point for 16-byte gathers
+    const double vol = p.xv[i].w;
+    if (!p.mixed) {
+      double2 *Mt = reinterpret_cast<double2 *>(p.Mt + 10 * i);
+      Mt[0] = make_double2(vol * M[0], vol * M[1]);
+      Mt[1] = make_double2(vol * M[2], vol * M[3]);
+      Mt[2] = make_double2(vol * M[4], vol * M[5]);
+      Mt[3] = make_double2(vol * M[6], vol * M[7]);
+      Mt[4] = make_double2(vol * M[8], 0.0);
+    } else {
+      float4 *Mf = reinterpret_cast<float4 *>(p.Mf + 12 * i);
+      Mf[0] = make_float4((float)(vol * M[0]), (float)(vol * M[1]), (float)(vol * M[2]),
+                          (float)(vol * M[3]));
+      Mf[1] = make_float4((float)(vol * M[4]), (float)(vol * M[5]), (float)(vol * M[6]),
+                          (float)(vol * M[7]));
+      Mf[2] = make_float4((float)(vol * M[8]), 0.f, 0.f, 0.f);
     }
 #pragma unroll
     for (int c = 0; c < 6; ++c) {
@@ -264,7 +293,6 @@ __global__ void __launch_bounds__(kMaterialThreads) k_material(StepParams p) {
     p.eP[i] = pt.eInelastic;
     // diagnostics: internal-energy increment with the reference's mixed-frame average
     // (BoundaryValueCaseRunner.cpp:231-238), observation-window means, max eqps, finiteness
-    const double vol = p.xv[i].w;
     const double a0 = 0.5 * (oldFull[0] + spatial[0]), a4 = 0.5 * (oldFull[4] + spatial[4]);
     const double a8 = 0.5 * (oldFull[8] + spatial[8]), a1 = 0.5 * (oldFull[1] + spatial[1]);
     const double a2 = 0.5 * (oldFull[2] + spatial[2]), a5 = 0.5 * (oldFull[5] + spatial[5]);
@@ -302,93 +330,107 @@ __global__ void __launch_bounds__(kMaterialThreads) k_material(StepParams p) {
   }
 }
 
-// ------------------------------------------------------------------ k_force
+// ------------------------------------------------------------------ k_force (sliced ELL)
+// Bond sum of the force density: f = M_i sum V_j xi + sum (V_j M_j) xi over intact bonds.
 __global__ void __launch_bounds__(kBondThreads) k_force(StepParams p) {
   const int64_t n = p.n;
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t nsl = (n + 31) >> 5;
+  if (i >= nsl * 32)
+    return;
+  const int64_t s = i >> 5;
+  const int lane = (int)(i & 31);
+  const bool valid = i < n;
+  const int64_t ii = valid ? i : 0;
+  const double4 xi = p.xv[ii];
+  const int len = valid ? p.len[i] : 0;
+  const int64_t off = p.slice_off[s];
+  const int width = (int)((p.slice_off[s + 1] - off) >> 5);
+  const int32_t *idx = p.sell + off + lane;
+  const uint32_t *words = p.words + (off >> 5);
+  double f0 = 0, f1 = 0, f2 = 0, s0 = 0, s1 = 0, s2 = 0;
+  for (int k = 0; k < width; ++k) {
+    const int32_t j = __ldg(idx + 32 * k);
+    const double4 xj = ldg4(p.xv + j);
+    const bool intact = k < len && !(p.damage && ((words[k] >> lane) & 1u));
+    const double w = intact ? xj.w : 0.0, g = intact ? 1.0 : 0.0;
+    const double e0 = xj.x - xi.x, e1 = xj.y - xi.y, e2 = xj.z - xi.z;
+    s0 += w * e0, s1 += w * e1, s2 += w * e2;
+    const double2 *Mj = reinterpret_cast<const double2 *>(p.Mt + 10 * (int64_t)j);
+    const double2 a = __ldg(Mj), b = __ldg(Mj + 1), c = __ldg(Mj + 2), d = __ldg(Mj + 3),
+                  h = __ldg(Mj + 4);
+    f0 += g * (a.x * e0 + a.y * e1 + b.x * e2);
+    f1 += g * (b.y * e0 + c.x * e1 + c.y * e2);
+    f2 += g * (d.x * e0 + d.y * e1 + h.x * e2);
+  }
+  if (!valid)
+    return;
+  const double *Mi = p.Mt + 10 * i;
+  const double rv = 1.0 / xi.w;  // M_i = (V_i M_i) / V_i
+  f0 += (Mi[0] * s0 + Mi[1] * s1 + Mi[2] * s2) * rv;
+  f1 += (Mi[3] * s0 + Mi[4] * s1 + Mi[5] * s2) * rv;
+  f2 += (Mi[6] * s0 + Mi[7] * s1 + Mi[8] * s2) * rv;
+  p.force[i] = make_double4(f0, f1, f2, 0.0);
+}
+
+// ------------------------------------------------------------------ k_integrate
+// Velocity-Verlet correction with the force density, constraints at t_n, diagnostics, then
+// the next increment's prediction with constraints at t_n+1; the last block writes the row.
+__global__ void __launch_bounds__(kBondThreads) k_integrate(StepParams p) {
+  const int64_t n = p.n;
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t step = *p.step;
   double part[PF_COUNT] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-  if (i < nsl * 32) {
-    const int64_t s = i >> 5;
-    const int lane = (int)(i & 31);
-    const bool valid = i < n;
-    const int64_t ii = valid ? i : 0;
-    const double4 xi = p.xv[ii];
-    const int len = valid ? p.len[i] : 0;
-    const int64_t off = p.slice_off[s];
-    const int width = (int)((p.slice_off[s + 1] - off) >> 5);
-    const int32_t *idx = p.sell + off + lane;
-    const uint32_t *words = p.words + (off >> 5);
-    double f0 = 0, f1 = 0, f2 = 0, s0 = 0, s1 = 0, s2 = 0;
-    for (int k = 0; k < width; ++k) {
-      const int32_t j = __ldg(idx + 32 * k);
-      const double4 xj = ldg4(p.xv + j);
-      const bool intact = k < len && !(p.damage && ((words[k] >> lane) & 1u));
-      const double w = intact ? xj.w : 0.0;
-      const double e0 = xj.x - xi.x, e1 = xj.y - xi.y, e2 = xj.z - xi.z;
-      s0 += w * e0, s1 += w * e1, s2 += w * e2;
-      const double *Mj = p.M + j;
-      const double t0 = __ldg(Mj) * e0 + __ldg(Mj + n) * e1 + __ldg(Mj + 2 * n) * e2;
-      const double t1 = __ldg(Mj + 3 * n) * e0 + __ldg(Mj + 4 * n) * e1 + __ldg(Mj + 5 * n) * e2;
-      const double t2 = __ldg(Mj + 6 * n) * e0 + __ldg(Mj + 7 * n) * e1 + __ldg(Mj + 8 * n) * e2;
-      f0 += w * t0, f1 += w * t1, f2 += w * t2;
-    }
-    if (valid) {
-      double Mi[9];
-#pragma unroll
-      for (int c = 0; c < 9; ++c)
-        Mi[c] = p.M[c * n + i];
-      f0 += Mi[0] * s0 + Mi[1] * s1 + Mi[2] * s2;
-      f1 += Mi[3] * s0 + Mi[4] * s1 + Mi[5] * s2;
-      f2 += Mi[6] * s0 + Mi[7] * s1 + Mi[8] * s2;
-      const double4 *Ucur = (step & 1) ? p.u1 : p.u0;
-      double4 *Unext = (step & 1) ? p.u0 : p.u1;
-      double4 u = Ucur[i], v = p.vel[i], a = p.acc[i];
-      const uint8_t fl = p.flags[i];
-      const double dt = p.dt, rho = p.rho;
-      double4 an = make_double4(f0 / rho, f1 / rho, f2 / rho, 0.0);
-      v.x += 0.5 * dt * (a.x + an.x);
-      v.y += 0.5 * dt * (a.y + an.y);
-      v.z += 0.5 * dt * (a.z + an.z);
-      a = an;
-      const double t = (double)step * dt;
-      double r[6];
+  if (i < n) {
+    const double4 fv = p.force[i];
+    const double f0 = fv.x, f1 = fv.y, f2 = fv.z;
+    const double4 *Ucur = (step & 1) ? p.u1 : p.u0;
+    double4 *Unext = (step & 1) ? p.u0 : p.u1;
+    double4 u = Ucur[i], v = p.vel[i], a = p.acc[i];
+    const uint8_t fl = p.flags[i];
+    const double dt = p.dt, rho = p.rho;
+    double4 an = make_double4(f0 / rho, f1 / rho, f2 / rho, 0.0);
+    v.x += 0.5 * dt * (a.x + an.x);
+    v.y += 0.5 * dt * (a.y + an.y);
+    v.z += 0.5 * dt * (a.z + an.z);
+    a = an;
+    const double t = (double)step * dt;
+    double r[6];
+    if (fl & (FLAG_SUPPORT | FLAG_LOADED))
+      ramp(p.bc, t, r);
+    apply_bc(p.bc, fl, r, u, v, a);
+    p.vel[i] = v;
+    p.acc[i] = a;
+    const double vol = p.xv[i].w;
+    part[PF_NETX] = f0 * vol, part[PF_NETY] = f1 * vol, part[PF_NETZ] = f2 * vol;
+    const double fax = p.bc.axis == 0 ? f0 : f1;
+    if (fl & FLAG_LOADED)
+      part[PF_REACTION] = (rho * r[2] - fax) * vol;
+    if (fl & FLAG_SUPPORT)
+      part[PF_SUPPORT_REACTION] = (rho * r[5] - fax) * vol;
+    part[PF_KINETIC] = 0.5 * rho * vol * (v.x * v.x + v.y * v.y + v.z * v.z);
+    const double ul = comp(u, p.bc.lateral);
+    if (fl & FLAG_LATERAL_POS)
+      part[PF_LAT_POS] = ul;
+    if (fl & FLAG_LATERAL_NEG)
+      part[PF_LAT_NEG] = ul;
+    part[PF_NONFINITE] = (isfinite(f0) && isfinite(f1) && isfinite(f2)) ? 0.0 : 1.0;
+    // predict the next increment (ExplicitTimeIntegrator.cpp:23-34) and constrain at t+dt
+    double4 un = make_double4(u.x + (dt * v.x + 0.5 * dt * dt * a.x),
+                              u.y + (dt * v.y + 0.5 * dt * dt * a.y),
+                              u.z + (dt * v.z + 0.5 * dt * dt * a.z), 0.0);
+    if (fl) {
+      double rn[6];
       if (fl & (FLAG_SUPPORT | FLAG_LOADED))
-        ramp(p.bc, t, r);
-      apply_bc(p.bc, fl, r, u, v, a);
-      p.vel[i] = v;
-      p.acc[i] = a;
-      p.force[i] = make_double4(f0, f1, f2, 0.0);
-      const double vol = xi.w;
-      part[PF_NETX] = f0 * vol, part[PF_NETY] = f1 * vol, part[PF_NETZ] = f2 * vol;
-      const double fax = p.bc.axis == 0 ? f0 : f1;
-      if (fl & FLAG_LOADED)
-        part[PF_REACTION] = (rho * r[2] - fax) * vol;
-      if (fl & FLAG_SUPPORT)
-        part[PF_SUPPORT_REACTION] = (rho * r[5] - fax) * vol;
-      part[PF_KINETIC] = 0.5 * rho * vol * (v.x * v.x + v.y * v.y + v.z * v.z);
-      const double ul = comp(u, p.bc.lateral);
-      if (fl & FLAG_LATERAL_POS)
-        part[PF_LAT_POS] = ul;
-      if (fl & FLAG_LATERAL_NEG)
-        part[PF_LAT_NEG] = ul;
-      part[PF_NONFINITE] = (isfinite(f0) && isfinite(f1) && isfinite(f2)) ? 0.0 : 1.0;
-      // predict the next increment (ExplicitTimeIntegrator.cpp:23-34) and constrain at t+dt
-      double4 un = make_double4(u.x + (dt * v.x + 0.5 * dt * dt * a.x),
-                                u.y + (dt * v.y + 0.5 * dt * dt * a.y),
-                                u.z + (dt * v.z + 0.5 * dt * dt * a.z), 0.0);
-      if (fl) {
-        double rn[6];
-        if (fl & (FLAG_SUPPORT | FLAG_LOADED))
-          ramp(p.bc, (double)(step + 1) * dt, rn);
-        double4 vv = v, aa = a;
-        apply_bc(p.bc, fl, rn, un, vv, aa);
-      }
-      if (p.bc.plane_strain)
-        un.z = 0.0;
-      Unext[i] = un;
+        ramp(p.bc, (double)(step + 1) * dt, rn);
+      double4 vv = v, aa = a;
+      apply_bc(p.bc, fl, rn, un, vv, aa);
     }
+    if (p.bc.plane_strain)
+      un.z = 0.0;
+    Unext[i] = un;
+    if (p.mixed)
+      p.uf[i] = make_float4((float)un.x, (float)un.y, (float)un.z, 0.0f);
   }
   block_partials<PF_COUNT>(part, p.part_force);
 
@@ -400,20 +442,42 @@ __global__ void __launch_bounds__(kBondThreads) k_force(StepParams p) {
   __syncthreads();
   if (!last)
     return;
+  // every thread folds a fixed strided subset of the block partials, then a fixed-order tree
+  // over the threads: deterministic, and the partial loads are spread over the whole block
+  double acc[PM_COUNT + PF_COUNT];
+#pragma unroll
+  for (int q = 0; q < PM_COUNT + PF_COUNT; ++q)
+    acc[q] = 0.0;
+  for (int b = threadIdx.x; b < p.mat_blocks; b += blockDim.x)
+#pragma unroll
+    for (int q = 0; q < PM_COUNT; ++q) {
+      const double v = __ldcg(p.part_mat + (size_t)b * PM_COUNT + q);
+      acc[q] = q == PM_MAX_EQPS ? fmax(acc[q], v) : acc[q] + v;
+    }
+  for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x)
+#pragma unroll
+    for (int q = 0; q < PF_COUNT; ++q)
+      acc[PM_COUNT + q] += __ldcg(p.part_force + (size_t)b * PF_COUNT + q);
+  __shared__ double red[kBondThreads / 32][PM_COUNT + PF_COUNT];
   __shared__ double tot[PM_COUNT + PF_COUNT];
+#pragma unroll
+  for (int q = 0; q < PM_COUNT + PF_COUNT; ++q)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double y = __shfl_xor_sync(0xffffffffu, acc[q], o);
+      acc[q] = q == PM_MAX_EQPS ? fmax(acc[q], y) : acc[q] + y;
+    }
+  if ((threadIdx.x & 31) == 0)
+#pragma unroll
+    for (int q = 0; q < PM_COUNT + PF_COUNT; ++q)
+      red[threadIdx.x >> 5][q] = acc[q];
+  __syncthreads();
   if (threadIdx.x < PM_COUNT + PF_COUNT) {
     const int q = threadIdx.x;
-    double acc = 0.0;
-    if (q < PM_COUNT) {
-      for (int b = 0; b < p.mat_blocks; ++b) {
-        const double v = __ldcg(p.part_mat + (size_t)b * PM_COUNT + q);
-        acc = q == PM_MAX_EQPS ? fmax(acc, v) : acc + v;
-      }
-    } else {
-      for (int b = 0; b < (int)gridDim.x; ++b)
-        acc += __ldcg(p.part_force + (size_t)b * PF_COUNT + (q - PM_COUNT));
-    }
-    tot[q] = acc;
+    double s = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w)
+      s = q == PM_MAX_EQPS ? fmax(s, red[w][q]) : s + red[w][q];
+    tot[q] = s;
   }
   __syncthreads();
   if (threadIdx.x != 0)
@@ -499,8 +563,9 @@ __global__ void k_init(StepParams p) {
     p.Fn[c * p.n + i] = id;
     p.Vn[c * p.n + i] = id;
     p.Rn[c * p.n + i] = id;
-    p.M[c * p.n + i] = 0.0;
   }
+  for (int c = 0; c < 10; ++c)
+    p.Mt[10 * i + c] = 0.0;
   for (int c = 0; c < 6; ++c)
     p.En[c * p.n + i] = 0.0, p.sig[c * p.n + i] = 0.0;
   for (int c = 0; c < p.nstatev; ++c)
@@ -558,13 +623,26 @@ int launch_shape_inverse_sell(const StepParams &p, cudaStream_t s) {
   return VPD_OK;
 }
 
+int integrate_grid(int64_t n) { return (int)((n + kBondThreads - 1) / kBondThreads); }
+
 int launch_stage(int stage, const StepParams &p, cudaStream_t s) {
-  if (stage == 0)
+  if (stage == 0) {
+    if (p.mixed)
+      return launch_deformation_mixed(p, s);
+    if (p.st.nw)
+      return launch_deformation_stencil(p, s);
     k_deformation<<<bond_grid(p.n), kBondThreads, 0, s>>>(p);
-  else if (stage == 1)
+  } else if (stage == 1) {
     k_material<<<(unsigned)material_grid(p.n), kMaterialThreads, 0, s>>>(p);
-  else
+  } else if (stage == 2) {
+    if (p.mixed)
+      return launch_force_mixed(p, s);
+    if (p.st.nw)
+      return launch_force_stencil(p, s);
     k_force<<<bond_grid(p.n), kBondThreads, 0, s>>>(p);
+  } else {
+    k_integrate<<<(unsigned)integrate_grid(p.n), kBondThreads, 0, s>>>(p);
+  }
   VPD_CUDA(cudaGetLastError());
   return VPD_OK;
 }

@@ -24,6 +24,18 @@ enum { ACC_INTERNAL = 0, ACC_EXTERNAL, ACC_PREV_POWER, ACC_FINITE, ACC_COUNT };
 constexpr int kDiagRing = 4096;      // diagnostic rows buffered on the device
 constexpr int kBondThreads = 256;    // threads per block of the bond kernels
 constexpr int kMaterialThreads = 128;
+constexpr int kMaxStencilWords = 32; // at most 1024 lattice offsets per stencil
+
+// Lattice-stencil bond layout (vpd_stencil.cu). nw == 0: not in use.
+struct StencilLayout {
+  int slots = 0, nw = 0;
+  int32_t *delta = nullptr;    // [32 nw] index difference j - i of each slot (0: padding)
+  int32_t *reverse = nullptr;  // [32 nw] slot of the opposite offset
+  uint32_t *forward = nullptr; // [nw] bits of the slots with delta > 0
+  uint32_t *mask = nullptr;    // [nw][n] bond bits
+  uint32_t *broken = nullptr;  // [nw][n] broken-bond bits
+  float4 *e0 = nullptr;        // [32 nw] lattice offset of each slot times h (mixed precision)
+};
 
 struct StepParams {
   int64_t n;
@@ -34,12 +46,21 @@ struct StepParams {
   const int64_t *slice_off;   // sliced-ELL slice offsets
   const int32_t *sell;        // sliced-ELL neighbour indices
   uint32_t *words;            // broken-bond bits, one word per (slice, column)
+  StencilLayout st;           // lattice-stencil layout; used instead of the ELL when st.nw > 0
   // kinematic state
   double4 *u0, *u1;           // displacement ping-pong: increment s reads u[s & 1]
   double4 *vel, *acc, *force;
   // material state, structure of arrays (component c of point i at [c * n + i])
   const double *kinv;
-  double *F, *Fn, *Vn, *Rn, *En, *sig, *state, *eI, *eP, *M;
+  double *F, *Fn, *Vn, *Rn, *En, *sig, *state, *eI, *eP;
+  double *Mt;                 // V_i M_i, 10 doubles per point (point-major)
+  // mixed precision (VPD_PRECISION_MIXED): FP32 copies gathered by the bond kernels
+  int mixed;
+  float4 *jit;                // (X_i - lattice position, V_i)
+  float4 *uf;                 // predicted displacement
+  float *Gf;                  // sum V_j (u_j - u_i) (x) xi, 9 floats structure of arrays
+  float *Mf;                  // V_i M_i, 12 floats per point
+  float tension2f, compression2f;
   int nstatev;
   // boundary and diagnostics sets
   const uint8_t *flags;
@@ -59,12 +80,29 @@ struct StepParams {
   double interior, gauge, lat_gauge, area, sign, n_lat_pos, n_lat_neg;
 };
 
-// The increment's kernels, in order: deformation (+ bond breaking), material, force.
-constexpr int kStages = 3;
+// The increment's kernels, in order: deformation (+ bond breaking), material, force bond sum,
+// integration (+ boundary conditions, diagnostics, next prediction).
+constexpr int kStages = 4;
 int launch_init(const StepParams &p, cudaStream_t s);
 int launch_stage(int stage, const StepParams &p, cudaStream_t s);
 int launch_increment(const StepParams &p, cudaStream_t s);
 int launch_shape_inverse_sell(const StepParams &p, cudaStream_t s);
 int material_grid(int64_t n);
+int integrate_grid(int64_t n);
+
+// lattice-stencil layout (vpd_stencil.cu): st.nw stays 0 when the points do not form the
+// lattice in index order or the stencil is too large
+int build_stencil(const int64_t *row_ptr, const int32_t *col, int64_t n, int ny, int nz,
+                  double spacing, StencilLayout &st, cudaStream_t s);
+void free_stencil(StencilLayout &st);
+int launch_shape_stencil(const StepParams &p, cudaStream_t s);
+int launch_deformation_stencil(const StepParams &p, cudaStream_t s);
+int launch_force_stencil(const StepParams &p, cudaStream_t s);
+int launch_damage_index_stencil(const StepParams &p, double *out, cudaStream_t s);
+// mixed precision (vpd_mixed.cu)
+int launch_deformation_mixed(const StepParams &p, cudaStream_t s);
+int launch_force_mixed(const StepParams &p, cudaStream_t s);
+int launch_mixed_setup(const StepParams &p, int ny, int nz, double h, double yoff, double zoff,
+                       cudaStream_t s);
 
 }  // namespace vpd

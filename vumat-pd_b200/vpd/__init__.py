@@ -68,6 +68,7 @@ def library():
     lib.vpd_num_points.argtypes = [_VP]
     lib.vpd_num_bonds.restype = ctypes.c_int64
     lib.vpd_num_bonds.argtypes = [_VP]
+    lib.vpd_bond_layout_words.argtypes = [_VP]
     lib.vpd_step.argtypes = [_VP, ctypes.c_int32, _D]
     lib.vpd_download.argtypes = [_VP, ctypes.c_int32, _D]
     lib.vpd_neighbors.argtypes = [_VP, _I64, _I32]
@@ -122,6 +123,11 @@ class Simulation:
     def n_bonds(self) -> int:
         return int(library().vpd_num_bonds(self._h))
 
+    @property
+    def layout_words(self) -> int:
+        """Lattice-stencil mask words per point (0: sliced-ELL index layout)."""
+        return int(library().vpd_bond_layout_words(self._h))
+
     def step(self, nsteps: int, diagnostics: bool = True) -> np.ndarray | None:
         """Advances nsteps increments; returns nsteps x 18 timeseries rows."""
         rows = np.zeros((nsteps, len(DIAG_COLUMNS))) if diagnostics else None
@@ -135,9 +141,9 @@ class Simulation:
 
     def profile_stages(self, nsteps: int) -> dict:
         """Advances nsteps increments with CUDA events between the kernels; mean ms each."""
-        out = np.zeros(3)
+        out = np.zeros(4)
         _check(library().vpd_profile_increment(self._h, nsteps, _dp(out)))
-        return dict(zip(("deformation", "material", "force"), out.tolist()))
+        return dict(zip(("deformation", "material", "force", "integrate"), out.tolist()))
 
     def field(self, name: str, out: np.ndarray | None = None) -> np.ndarray:
         width = self.case.nstatev if name == "state" else FIELD_WIDTH[name]
