@@ -337,7 +337,7 @@ int create_impl(vpd_handle *h, const vpd_case *c, const double *positions, const
       (rc = dalloc(h, &h->Fn, 9 * n)) || (rc = dalloc(h, &h->Vn, 9 * n)) ||
       (rc = dalloc(h, &h->Rn, 9 * n)) || (rc = dalloc(h, &h->En, 6 * n)) ||
       (rc = dalloc(h, &h->sig, 6 * n)) || (rc = dalloc(h, &h->state, (size_t)c->nstatev * n)) ||
-      (rc = dalloc(h, &h->eI, n)) || (rc = dalloc(h, &h->eP, n)) || (rc = dalloc(h, &h->Mt, 10 * n)) ||
+      (rc = dalloc(h, &h->eI, n)) || (rc = dalloc(h, &h->eP, n)) ||
       (rc = dalloc(h, &h->obsw, n)) || (rc = dalloc(h, &h->flags, n)) ||
       (rc = dalloc(h, &h->row_ptr, n + 1)) || (rc = dalloc(h, &h->step_dev, 1)) ||
       (rc = dalloc(h, &h->status_dev, 1)) || (rc = dalloc(h, &h->counter, 1)) ||
@@ -395,7 +395,7 @@ int create_impl(vpd_handle *h, const vpd_case *c, const double *positions, const
     h->allocations.push_back(h->len);
     h->allocations.push_back(h->slice_off);
     h->allocations.push_back(h->sell);
-    if ((rc = dalloc(h, &h->words, (size_t)(h->sell_total / 32))))
+    if ((rc = dalloc(h, &h->words, (size_t)(h->sell_total / 32))) || (rc = dalloc(h, &h->Mt, 10 * n)))
       return rc;
     VPD_CUDA(cudaMemsetAsync(h->words, 0, sizeof(uint32_t) * std::max<int64_t>(h->sell_total / 32, 1), s));
   }
@@ -415,6 +415,9 @@ int create_impl(vpd_handle *h, const vpd_case *c, const double *positions, const
   p.kinv = h->kinv, p.F = h->F, p.Fn = h->Fn, p.Vn = h->Vn, p.Rn = h->Rn, p.En = h->En;
   p.sig = h->sig, p.state = h->state, p.eI = h->eI, p.eP = h->eP, p.Mt = h->Mt;
   p.st = h->st;
+  if (p.st.nw && ((rc = dalloc(h, &p.vxi, n)) ||
+                  (c->precision != VPD_PRECISION_MIXED && (rc = dalloc(h, &p.fmap, 3 * n)))))
+    return rc;
   p.nstatev = c->nstatev;
   p.flags = h->flags, p.obsw = h->obsw;
   p.jc = make_jc_params(c->props);
@@ -433,7 +436,7 @@ int create_impl(vpd_handle *h, const vpd_case *c, const double *positions, const
                        "mixed precision needs the points in lattice order (lattice-stencil bonds)");
     float4 *jit = nullptr;
     if ((rc = dalloc(h, &jit, n)) || (rc = dalloc(h, &p.uf, n)) || (rc = dalloc(h, &p.Gf, 9 * n)) ||
-        (rc = dalloc(h, &p.Mf, 12 * n)))
+        (rc = dalloc(h, &p.fmapf, 3 * n)))
       return rc;
     p.jit = jit;
     p.mixed = 1;

@@ -11,6 +11,20 @@
 
 namespace vpd {
 
+// 32-byte global load through the read-only path and 32-byte store (sm_100 vector width);
+// the address must be 32-byte aligned (every double4 array here is). A warp reading
+// consecutive double4 elements then touches each 32-byte sector once, where two 16-byte
+// halves would touch every sector twice.
+__device__ __forceinline__ double4 ldg256(const double4 *p) {
+  double4 r;
+  asm("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];" : "=d"(r.x), "=d"(r.y), "=d"(r.z), "=d"(r.w) : "l"(p));
+  return r;
+}
+__device__ __forceinline__ void st256(double4 *p, double4 v) {
+  asm volatile("st.global.v4.f64 [%0], {%1,%2,%3,%4};" ::"l"(p), "d"(v.x), "d"(v.y), "d"(v.z), "d"(v.w)
+               : "memory");
+}
+
 __device__ __forceinline__ void m_mul(const double *a, const double *b, double *o) {
 #pragma unroll
   for (int i = 0; i < 3; ++i)

@@ -4,7 +4,7 @@
 //   jit[i] = (X_i - lattice_i, V_i) as float4, so a bond vector is
 //            xi = (o h) + (jit_j - jit_i) with the slot's lattice offset o h (float, per slot);
 //   uf[i]  = the predicted displacement as float4, written by the integrator;
-//   Mf[i]  = V_i M_i (force map scaled by volume) as 12 floats (three float4).
+//   fmapf[r * n + i] = row r of V_i M_i (force map scaled by volume) with jit_i's component r.
 // Each 32-slot word is summed in plain FP32 and the word sums are added with Kahan
 // compensation, so the result carries ~1 FP32 ulp of error (relative ~6e-8) rather than the
 // bond count times it. FP64 stays where the update integrates: K^-1, F = I + G K^-1, the
@@ -127,51 +127,60 @@ __global__ void __launch_bounds__(kBondThreads, 3) k_deformation_mixed(StepParam
     p.Gf[c * n + i] = Gs[c];
 }
 
-// f = M_i sum V_j xi + sum (V_j M_j) xi over intact bonds, in FP32 with Kahan-folded words.
+// f = sum (V_j M_j) xi over intact bonds + M_i s_i with s_i = vxi_i - sum_{broken j} V_j xi.
+// A bond reads the three FP32 force-map records of j (the jitter offset rides in their fourth
+// lane); the bond sum is FP32 with Kahan-folded words, s_i and the M_i term are FP64.
 __global__ void __launch_bounds__(kBondThreads, 3) k_force_mixed(StepParams p) {
   const int64_t n = p.n;
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const bool valid = i < n;
   const int64_t ii = valid ? i : n - 1;
   const float4 ji = ldgf4(p.jit + ii);
-  float fs[3] = {0, 0, 0}, fc[3] = {0, 0, 0}, ss[3] = {0, 0, 0}, sc[3] = {0, 0, 0};
+  const float4 *P0 = p.fmapf, *P1 = p.fmapf + n, *P2 = p.fmapf + 2 * n;
+  float fs[3] = {0, 0, 0}, fc[3] = {0, 0, 0};
+  double c0 = 0, c1 = 0, c2 = 0;
   for (int w = 0; w < p.st.nw; ++w) {
     uint32_t m = valid ? __ldg(p.st.mask + (int64_t)w * n + i) : 0u;
-    if (p.damage)
-      m &= ~p.st.broken[(int64_t)w * n + ii];
-    if (__all_sync(0xffffffffu, m == 0u))
-      continue;
     const int32_t *dl = p.st.delta + 32 * w;
     const float4 *ol = p.st.e0 + 32 * w;
-    float f0 = 0, f1 = 0, f2 = 0, s0 = 0, s1 = 0, s2 = 0;
+    if (p.damage) {
+      const uint32_t bk = m & p.st.broken[(int64_t)w * n + ii];
+      for (uint32_t f = bk; f; f &= f - 1) {  // broken bonds leave s_i
+        const int b = __ffs(f) - 1;
+        const float4 jj = p.jit[i + dl[b]], o = ol[b];
+        c0 += (double)(jj.w * (o.x + (jj.x - ji.x)));
+        c1 += (double)(jj.w * (o.y + (jj.y - ji.y)));
+        c2 += (double)(jj.w * (o.z + (jj.z - ji.z)));
+      }
+      m &= ~bk;
+    }
+    if (__all_sync(0xffffffffu, m == 0u))
+      continue;
+    float f0 = 0, f1 = 0, f2 = 0;
 #pragma unroll 4
     for (int b = 0; b < 32; ++b) {
       const bool bond = (m >> b) & 1u;
       const int64_t j = clamp_index(ii + __ldg(dl + b), n);  // contiguous across the warp
       const float4 o = __ldg(ol + b);
-      const float4 jj = ldgf4(p.jit + j);
-      const float e0 = bond ? o.x + (jj.x - ji.x) : 0.0f;
-      const float e1 = bond ? o.y + (jj.y - ji.y) : 0.0f;
-      const float e2 = bond ? o.z + (jj.z - ji.z) : 0.0f;
-      s0 += jj.w * e0, s1 += jj.w * e1, s2 += jj.w * e2;
-      const float4 *Mj = reinterpret_cast<const float4 *>(p.Mf + 12 * j);
-      const float4 a = __ldg(Mj), c = __ldg(Mj + 1), d = __ldg(Mj + 2);
+      const float4 a = ldgf4(P0 + j), c = ldgf4(P1 + j), d = ldgf4(P2 + j);
+      const float e0 = bond ? o.x + (a.w - ji.x) : 0.0f;
+      const float e1 = bond ? o.y + (c.w - ji.y) : 0.0f;
+      const float e2 = bond ? o.z + (d.w - ji.z) : 0.0f;
       f0 += a.x * e0 + a.y * e1 + a.z * e2;
-      f1 += a.w * e0 + c.x * e1 + c.y * e2;
-      f2 += c.z * e0 + c.w * e1 + d.x * e2;
+      f1 += c.x * e0 + c.y * e1 + c.z * e2;
+      f2 += d.x * e0 + d.y * e1 + d.z * e2;
     }
     kahan_add(fs[0], fc[0], f0), kahan_add(fs[1], fc[1], f1), kahan_add(fs[2], fc[2], f2);
-    kahan_add(ss[0], sc[0], s0), kahan_add(ss[1], sc[1], s1), kahan_add(ss[2], sc[2], s2);
   }
   if (!valid)
     return;
-  const float4 *Mi4 = reinterpret_cast<const float4 *>(p.Mf + 12 * i);
-  const float4 a = Mi4[0], c = Mi4[1], d = Mi4[2];
+  const float4 a = P0[i], c = P1[i], d = P2[i];
+  const double4 s = p.vxi[i];
+  const double s0 = s.x - c0, s1 = s.y - c1, s2 = s.z - c2;
   const double rv = 1.0 / (double)ji.w;
-  const double s0 = ss[0], s1 = ss[1], s2 = ss[2];
   const double f0 = (double)fs[0] + (a.x * s0 + a.y * s1 + a.z * s2) * rv;
-  const double f1 = (double)fs[1] + (a.w * s0 + c.x * s1 + c.y * s2) * rv;
-  const double f2 = (double)fs[2] + (c.z * s0 + c.w * s1 + d.x * s2) * rv;
+  const double f1 = (double)fs[1] + (c.x * s0 + c.y * s1 + c.z * s2) * rv;
+  const double f2 = (double)fs[2] + (d.x * s0 + d.y * s1 + d.z * s2) * rv;
   p.force[i] = make_double4(f0, f1, f2, 0.0);
 }
 

@@ -22,12 +22,6 @@
 
 namespace vpd {
 
-__device__ __forceinline__ double4 ldg4s(const double4 *p) {
-  const double2 *q = reinterpret_cast<const double2 *>(p);
-  const double2 a = __ldg(q), b = __ldg(q + 1);
-  return make_double4(a.x, a.y, b.x, b.y);
-}
-
 __device__ __forceinline__ int64_t clamp_index(int64_t j, int64_t n) {
   return j < 0 ? 0 : (j >= n ? n - 1 : j);
 }
@@ -212,7 +206,7 @@ __global__ void __launch_bounds__(kBondThreads) k_shape_stencil(StepParams p) {
   if (i >= n)
     return;
   const double4 xi = p.xv[i];
-  double K[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  double K[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, s[3] = {0, 0, 0};
   for (int w = 0; w < p.st.nw; ++w) {
     const uint32_t m = p.st.mask[(int64_t)w * n + i];
     for (int b = 0; b < 32; ++b)
@@ -220,12 +214,15 @@ __global__ void __launch_bounds__(kBondThreads) k_shape_stencil(StepParams p) {
         const double4 xj = p.xv[i + p.st.delta[32 * w + b]];
         const double e[3] = {xj.x - xi.x, xj.y - xi.y, xj.z - xi.z};
 #pragma unroll
-        for (int a = 0; a < 3; ++a)
+        for (int a = 0; a < 3; ++a) {
+          s[a] += xj.w * e[a];
 #pragma unroll
           for (int c = 0; c < 3; ++c)
             K[3 * a + c] += xj.w * e[a] * e[c];
+        }
       }
   }
+  p.vxi[i] = make_double4(s[0], s[1], s[2], 0.0);
   double Kinv[9];
   if (!m_inv(K, Kinv)) {
     atomicOr(p.status, STATUS_SINGULAR_K);
@@ -267,7 +264,7 @@ __global__ void __launch_bounds__(kBondThreads, DAMAGE ? 2 : 3) k_deformation_st
   const int64_t ii = valid ? i : n - 1;
   const int64_t step = *p.step;
   const double4 *U = (step & 1) ? p.u1 : p.u0;
-  const double4 xi = ldg4s(p.xv + ii), ui = ldg4s(U + ii);
+  const double4 xi = ldg256(p.xv + ii), ui = ldg256(U + ii);
   double G[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   const double lo = 1.0 - 1.0e-9, hi = 1.0 + 1.0e-9;
   for (int w = 0; w < p.st.nw; ++w) {
@@ -283,7 +280,7 @@ __global__ void __launch_bounds__(kBondThreads, DAMAGE ? 2 : 3) k_deformation_st
       // every lane reads i + delta (clamped), so the warp's loads stay one contiguous range;
       // lanes without this bond are masked by a zero weight
       const int64_t j = clamp_index(ii + __ldg(dl + b), n);
-      const double4 xj = ldg4s(p.xv + j), uj = ldg4s(U + j);
+      const double4 xj = ldg256(p.xv + j), uj = ldg256(U + j);
       const double v = ((m >> b) & 1u) ? xj.w : 0.0;
       const double e0 = xj.x - xi.x, e1 = xj.y - xi.y, e2 = xj.z - xi.z;
       const double d0 = uj.x - ui.x, d1 = uj.y - ui.y, d2 = uj.z - ui.z;
@@ -333,45 +330,52 @@ __global__ void __launch_bounds__(kBondThreads, DAMAGE ? 2 : 3) k_deformation_st
     p.F[c * n + i] = ((c % 4 == 0) ? 1.0 : 0.0) + GK[c];
 }
 
-// Bond sum of the force density over intact bonds: f = M_i sum V_j xi + sum (V_j M_j) xi.
+// Bond sum of the force density over intact bonds,
+//   f_i = sum_j V_j M_j xi + M_i s_i,   s_i = sum_j V_j xi = vxi_i - sum_{broken j} V_j xi,
+// so a bond reads only the three force-map records of j (its coordinates ride in their fourth
+// lane); broken bonds, rare, are taken out of the precomputed s_i one by one.
 // Writes f into p.force; the integrator runs in k_integrate (vpd_step.cu).
 __global__ void __launch_bounds__(kBondThreads, 3) k_force_stencil(StepParams p) {
   const int64_t n = p.n;
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const bool valid = i < n;
   const int64_t ii = valid ? i : n - 1;
-  const double4 xi = ldg4s(p.xv + ii);
-  double f0 = 0, f1 = 0, f2 = 0, s0 = 0, s1 = 0, s2 = 0;
+  const double4 xi = ldg256(p.xv + ii);
+  const double4 *P0 = p.fmap, *P1 = p.fmap + n, *P2 = p.fmap + 2 * n;
+  double f0 = 0, f1 = 0, f2 = 0, c0 = 0, c1 = 0, c2 = 0;
   for (int w = 0; w < p.st.nw; ++w) {
     uint32_t m = valid ? __ldg(p.st.mask + (int64_t)w * n + i) : 0u;
-    if (p.damage)
-      m &= ~p.st.broken[(int64_t)w * n + ii];
+    const int32_t *dl = p.st.delta + 32 * w;
+    if (p.damage) {
+      const uint32_t bk = m & p.st.broken[(int64_t)w * n + ii];
+      for (uint32_t f = bk; f; f &= f - 1) {  // broken bonds leave s_i
+        const double4 xj = p.xv[i + dl[__ffs(f) - 1]];
+        c0 += xj.w * (xj.x - xi.x), c1 += xj.w * (xj.y - xi.y), c2 += xj.w * (xj.z - xi.z);
+      }
+      m &= ~bk;
+    }
     if (__all_sync(0xffffffffu, m == 0u))
       continue;
-    const int32_t *dl = p.st.delta + 32 * w;
 #pragma unroll 4
     for (int b = 0; b < 32; ++b) {
       const bool bond = (m >> b) & 1u;
       const int64_t j = clamp_index(ii + __ldg(dl + b), n);  // contiguous across the warp
-      const double4 xj = ldg4s(p.xv + j);
-      const double e0 = bond ? xj.x - xi.x : 0.0, e1 = bond ? xj.y - xi.y : 0.0,
-                   e2 = bond ? xj.z - xi.z : 0.0;
-      s0 += xj.w * e0, s1 += xj.w * e1, s2 += xj.w * e2;
-      const double2 *Mj = reinterpret_cast<const double2 *>(p.Mt + 10 * j);
-      const double2 a = __ldg(Mj), b2 = __ldg(Mj + 1), c = __ldg(Mj + 2), d = __ldg(Mj + 3),
-                    g = __ldg(Mj + 4);
-      f0 += a.x * e0 + a.y * e1 + b2.x * e2;
-      f1 += b2.y * e0 + c.x * e1 + c.y * e2;
-      f2 += d.x * e0 + d.y * e1 + g.x * e2;
+      const double4 a = ldg256(P0 + j), c = ldg256(P1 + j), d = ldg256(P2 + j);
+      const double e0 = bond ? a.w - xi.x : 0.0, e1 = bond ? c.w - xi.y : 0.0,
+                   e2 = bond ? d.w - xi.z : 0.0;
+      f0 += a.x * e0 + a.y * e1 + a.z * e2;
+      f1 += c.x * e0 + c.y * e1 + c.z * e2;
+      f2 += d.x * e0 + d.y * e1 + d.z * e2;
     }
   }
   if (!valid)
     return;
-  const double *Mi = p.Mt + 10 * i;
+  const double4 a = P0[i], c = P1[i], d = P2[i], s = p.vxi[i];
+  const double s0 = s.x - c0, s1 = s.y - c1, s2 = s.z - c2;
   const double rv = 1.0 / xi.w;  // M_i = (V_i M_i) / V_i
-  f0 += (Mi[0] * s0 + Mi[1] * s1 + Mi[2] * s2) * rv;
-  f1 += (Mi[3] * s0 + Mi[4] * s1 + Mi[5] * s2) * rv;
-  f2 += (Mi[6] * s0 + Mi[7] * s1 + Mi[8] * s2) * rv;
+  f0 += (a.x * s0 + a.y * s1 + a.z * s2) * rv;
+  f1 += (c.x * s0 + c.y * s1 + c.z * s2) * rv;
+  f2 += (d.x * s0 + d.y * s1 + d.z * s2) * rv;
   p.force[i] = make_double4(f0, f1, f2, 0.0);
 }
 

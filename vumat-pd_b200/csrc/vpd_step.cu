@@ -266,22 +266,28 @@ __global__ void __launch_bounds__(kMaterialThreads) k_material(StepParams p) {
       p.Vn[c * n + i] = co.v[c];
       p.Rn[c * n + i] = co.r[c];
     }
-    // the force map scaled by the point's volume, 10 doubles per point for 16-byte gathers
-    const double vol = p.xv[i].w;
-    if (!p.mixed) {
+    // the force map scaled by the point's volume, in the layout the force kernel gathers
+    const double4 xi = p.xv[i];
+    const double vol = xi.w;
+    if (p.mixed) {
+      const float4 ji = p.jit[i];
+      const float jr[3] = {ji.x, ji.y, ji.z};
+#pragma unroll
+      for (int r = 0; r < 3; ++r)
+        p.fmapf[r * n + i] = make_float4((float)(vol * M[3 * r]), (float)(vol * M[3 * r + 1]),
+                                         (float)(vol * M[3 * r + 2]), jr[r]);
+    } else if (p.fmap) {
+      const double xr[3] = {xi.x, xi.y, xi.z};
+#pragma unroll
+      for (int r = 0; r < 3; ++r)
+        st256(p.fmap + r * n + i, make_double4(vol * M[3 * r], vol * M[3 * r + 1], vol * M[3 * r + 2], xr[r]));
+    } else {
       double2 *Mt = reinterpret_cast<double2 *>(p.Mt + 10 * i);
       Mt[0] = make_double2(vol * M[0], vol * M[1]);
       Mt[1] = make_double2(vol * M[2], vol * M[3]);
       Mt[2] = make_double2(vol * M[4], vol * M[5]);
       Mt[3] = make_double2(vol * M[6], vol * M[7]);
       Mt[4] = make_double2(vol * M[8], 0.0);
-    } else {
-      float4 *Mf = reinterpret_cast<float4 *>(p.Mf + 12 * i);
-      Mf[0] = make_float4((float)(vol * M[0]), (float)(vol * M[1]), (float)(vol * M[2]),
-                          (float)(vol * M[3]));
-      Mf[1] = make_float4((float)(vol * M[4]), (float)(vol * M[5]), (float)(vol * M[6]),
-                          (float)(vol * M[7]));
-      Mf[2] = make_float4((float)(vol * M[8]), 0.f, 0.f, 0.f);
     }
 #pragma unroll
     for (int c = 0; c < 6; ++c) {
@@ -564,8 +570,9 @@ __global__ void k_init(StepParams p) {
     p.Vn[c * p.n + i] = id;
     p.Rn[c * p.n + i] = id;
   }
-  for (int c = 0; c < 10; ++c)
-    p.Mt[10 * i + c] = 0.0;
+  if (p.Mt)
+    for (int c = 0; c < 10; ++c)
+      p.Mt[10 * i + c] = 0.0;
   for (int c = 0; c < 6; ++c)
     p.En[c * p.n + i] = 0.0, p.sig[c * p.n + i] = 0.0;
   for (int c = 0; c < p.nstatev; ++c)

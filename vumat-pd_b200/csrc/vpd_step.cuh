@@ -53,13 +53,17 @@ struct StepParams {
   // material state, structure of arrays (component c of point i at [c * n + i])
   const double *kinv;
   double *F, *Fn, *Vn, *Rn, *En, *sig, *state, *eI, *eP;
-  double *Mt;                 // V_i M_i, 10 doubles per point (point-major)
+  double *Mt;                 // V_i M_i, 10 doubles per point (point-major; sliced ELL only)
+  // lattice-stencil force map: row r of V_i M_i with the point's coordinate r,
+  // fmap[r * n + i] = (VM_r0, VM_r1, VM_r2, X_r), so one bond reads three 32-byte records
+  double4 *fmap;
+  double4 *vxi;               // sum over all bonds of V_j xi (FP64, set once; stencil layout)
   // mixed precision (VPD_PRECISION_MIXED): FP32 copies gathered by the bond kernels
   int mixed;
   float4 *jit;                // (X_i - lattice position, V_i)
   float4 *uf;                 // predicted displacement
   float *Gf;                  // sum V_j (u_j - u_i) (x) xi, 9 floats structure of arrays
-  float *Mf;                  // V_i M_i, 12 floats per point
+  float4 *fmapf;              // fmapf[r * n + i] = (VM_r0, VM_r1, VM_r2, jit_r) in FP32
   float tension2f, compression2f;
   int nstatev;
   // boundary and diagnostics sets

@@ -106,14 +106,18 @@ __device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
 
 // Warp-collective: each thread reads 16 consecutive FP32 columns of its TMEM lane
 // (lane = 32 * warp-in-quadrant + lane id; taddr carries the warp's lane base in bits 16+).
+// The load and its wait are one asm statement: tcgen05.ld writes its registers
+// asynchronously, and with a separate wait the compiler may move uses of the registers above
+// the wait (nothing ties them to it).
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *out) {
   uint32_t r[16];
   asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n\t"
+      "tcgen05.wait::ld.sync.aligned;"
       : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
         "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-      : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      : "r"(taddr)
+      : "memory");
 #pragma unroll
   for (int c = 0; c < 16; ++c)
     out[c] = __uint_as_float(r[c]);

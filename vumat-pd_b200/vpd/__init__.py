@@ -88,6 +88,8 @@ def library():
     lib.vpd_material_update.argtypes = [ctypes.c_int64, _D, ctypes.c_int32, ctypes.c_double] + [_VP] * 12
     lib.vpd_damage_update.argtypes = [_VP, _VP, _VP, ctypes.c_int64, _VP, _VP, ctypes.c_double,
                                       ctypes.c_double, _VP, _VP, _VP]
+    lib.vpd_mlp_forward.argtypes = [_VP, _VP, _VP, ctypes.c_int64, _VP, _VP]
+    lib.vpd_mlp_gradients.argtypes = [_VP, _VP, _VP, _VP, ctypes.c_int64, _VP, _VP]
     _lib = lib
     return lib
 
@@ -273,6 +275,29 @@ def material_update(props, dt, defgrad_new, state):
         _ptr(s["stress_corotational"]), _ptr(s["state"]), _ptr(s["temperature"]),
         _ptr(s["energy_internal"]), _ptr(s["energy_inelastic"]), _ptr(spatial), _stream()))
     return spatial
+
+
+def mlp_forward(weight_bits, biases, x):
+    """Surrogate network forward on the tensor cores: weight_bits int16/uint16 CUDA tensor
+    [VPD_MLP_WEIGHTS] (bf16 bit patterns), biases float32 [400], x float32 [B,16] -> [B,16]."""
+    import torch
+    out = torch.empty((x.shape[0], 16), dtype=torch.float32, device=x.device)
+    _check(library().vpd_mlp_forward(_ptr(weight_bits), _ptr(biases), _ptr(x), x.shape[0],
+                                     _ptr(out), _stream()))
+    return out
+
+
+def mlp_gradients(weight_bits, biases, x, gout):
+    """d/dparams of sum(network(x) * gout) -> float32 [VPD_MLP_PARAMS] (weights, then biases)."""
+    import torch
+    grad = torch.empty(MLP_PARAMS, dtype=torch.float32, device=x.device)
+    _check(library().vpd_mlp_gradients(_ptr(weight_bits), _ptr(biases), _ptr(x), _ptr(gout),
+                                       x.shape[0], _ptr(grad), _stream()))
+    return grad
+
+
+MLP_WEIGHTS = 36864
+MLP_PARAMS = 37264
 
 
 def damage_update(positions, displacement, volumes, row_ptr, col, initiation, failure,

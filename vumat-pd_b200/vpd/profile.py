@@ -1,0 +1,53 @@
+"""Per-stage timing of the increment on one tensile-bar workload (CUDA events on the handle's
+stream), for profiling runs:
+
+    python -m vpd.profile --config 3 --nx 100 --precision mixed --warm 2 --steps 4
+
+Prints one JSON line: points, bonds, layout words, ms per increment over --steps graph
+increments, and the four stage times (deformation, material, force, integrate) averaged over
+--stage-steps separately launched increments. Under a kernel profiler, --steps 0 and
+--stage-steps 1 keep the number of launches small.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import sys
+
+sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+
+import vpd  # noqa: E402
+from vpd.case import tensile_bar  # noqa: E402
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--config", type=int, default=3)
+    ap.add_argument("--nx", type=int, default=100)
+    ap.add_argument("--precision", choices=("fp64", "mixed"), default="fp64")
+    ap.add_argument("--no-damage", action="store_true")
+    ap.add_argument("--warm", type=int, default=2, help="untimed increments first")
+    ap.add_argument("--steps", type=int, default=4)
+    ap.add_argument("--stage-steps", type=int, default=3)
+    a = ap.parse_args(argv)
+    over = {"nx": a.nx, "precision": 1 if a.precision == "mixed" else 0}
+    if a.no_damage:
+        over["damage_mode"] = 0
+    case = tensile_bar(a.config, **over)
+    with vpd.Simulation(case) as sim:
+        if a.warm:
+            sim.step(a.warm, diagnostics=False)
+        ms = None
+        if a.steps:
+            sim.step(a.steps, diagnostics=False)
+            ms = sim.last_step_ms() / a.steps
+        stages = sim.profile_stages(a.stage_steps) if a.stage_steps else {}
+        print(json.dumps({"config": a.config, "nx": a.nx, "precision": a.precision,
+                          "damage": not a.no_damage, "points": sim.n_points, "bonds": sim.n_bonds,
+                          "layout_words": sim.layout_words, "ms_per_increment": ms,
+                          "stage_ms": stages}))
+
+
+if __name__ == "__main__":
+    main()
