@@ -128,6 +128,8 @@ enum {
   VPD_DIAG_ENERGY_ERROR,
   VPD_DIAG_NET_INTERNAL_FORCE,
   VPD_DIAG_FINITE,
+  VPD_DIAG_PLASTIC_POINTS,   /* points whose return map gave a plastic increment (state 5 > 0) */
+  VPD_DIAG_FALLBACK_POINTS,  /* surrogate mode: plastic points the gate sent to the VUMAT */
   VPD_DIAG_COLS
 };
 
@@ -258,6 +260,66 @@ int vpd_mlp_forward(const uint16_t *weights, const float *biases, const float *x
    backward pass for the output gradient gout [batch][16]. Synchronises the stream. */
 int vpd_mlp_gradients(const uint16_t *weights, const float *biases, const float *x,
                       const float *gout, int64_t batch, float *grad, void *stream);
+
+/* ---- the learned Johnson-Cook update (no reference counterpart) ----
+   Features and targets of one material-point increment (host arrays, 16 floats per row), with
+   deq the equivalent deviatoric strain increment and xf = (qTrial - oldYield) / (3 mu) the
+   increment of a return to the old yield stress (an upper bound of the plastic increment):
+   features 0-5 strain increment / deq, 6 (log10 eqps + 3) / 3, 7 (log10(deq / dt in 1/s)
+   - 1.5) / 3, 8 homologous temperature, 9 xf / deq (trial overstress, in [-2, 2]); targets
+   0 the plastic increment / xf (in (0, 1]), 1-6 stress increment / (2 mu deq), 15 the row's
+   training weight (1 when the trial state yields, else 0). */
+#define VPD_SURROGATE_MAX_EPOCHS 64
+#define VPD_SAMPLE_RECORD 26
+typedef struct vpd_surrogate_config {
+  double props[14];            /* Johnson-Cook properties, as vpd_case.props */
+  int64_t samples;             /* increments generated by the device VUMAT */
+  int32_t epochs;              /* 1 .. VPD_SURROGATE_MAX_EPOCHS */
+  int32_t batch;               /* rows per Adam step (>= 128) */
+  double learning_rate;        /* Adam */
+  uint64_t seed;
+  double validation_fraction;  /* held-out tail of the samples, [0, 0.5] */
+} vpd_surrogate_config;
+
+typedef struct vpd_surrogate_report {
+  int32_t epochs_run;
+  double epoch_loss[VPD_SURROGATE_MAX_EPOCHS]; /* mean weighted MSE of each epoch */
+  double validation_loss;
+  double ratio_rmse;           /* plastic validation rows: rms error of target 0 */
+  double stress_rmse;          /* plastic validation rows: rms error of targets 1-6 */
+  double plastic_fraction;     /* of all samples */
+  double train_ms;             /* device time of the training loop */
+} vpd_surrogate_report;
+
+/* Generates `count` increments with the device VUMAT (seeded; strain increments N(0, 1e-4)
+   per component for even rows, log-uniform magnitude 1e-8..1e-3 for odd rows; eqps
+   log-uniform [1e-6, 0.5]; strain rate log-uniform [1e-3, 1e4] /s; T uniform [293, 1200] K;
+   old stress on or inside the yield surface). features / targets: [count][16] floats;
+   records (may be NULL): [count][VPD_SAMPLE_RECORD] doubles: strain increment (6), old stress
+   (6), eqps, temperature, old yield stress, dt, new stress (6), plastic increment, bisection
+   iterations (cold start), trial yields (0/1), yield stress at zero increment. Host buffers. */
+int vpd_surrogate_samples(const double *props, uint64_t seed, int64_t count, float *features,
+                          float *targets, double *records);
+
+/* Generates cfg->samples increments with the device VUMAT and trains the network on them
+   with the tensor-core forward/backward kernels and Adam (weighted MSE, target 0 weighted 4).
+   weights [VPD_MLP_WEIGHTS] bf16 bits and biases [400] receive the trained parameters;
+   report (may be NULL) the losses and validation errors. */
+int vpd_train_surrogate(const vpd_surrogate_config *cfg, uint16_t *weights, float *biases,
+                        vpd_surrogate_report *report);
+
+enum { VPD_GUESS_NETWORK = 0, VPD_GUESS_WARM_START = 1, VPD_GUESS_HYBRID = 2 };
+/* Attaches the surrogate to a handle created with material_mode VPD_MATERIAL_SURROGATE:
+   each yielding point's plastic increment starts from the network's prediction
+   (VPD_GUESS_NETWORK; weights and biases as above, host arrays), from the point's previous
+   plastic increment (VPD_GUESS_WARM_START; weights may be NULL), or from the previous plastic
+   increment where the previous increment was plastic and the network elsewhere
+   (VPD_GUESS_HYBRID), takes at most newton_steps Newton steps (in ln of the increment) and is
+   accepted when the residual is below the VUMAT's tolerance E 1e-9; the
+   other points fall back to the VUMAT's bisection (VPD_DIAG_FALLBACK_POINTS). Required before
+   the first vpd_step of such a handle. */
+int vpd_set_surrogate(vpd_handle *h, const uint16_t *weights, const float *biases, int32_t guess,
+                      int32_t newton_steps);
 
 /* Plugin ABI: the Johnson-Cook VUMAT evaluated on the GPU for one block of host arrays
    in the reference's column-major [component][nblock] layout. Synchronous. A failure is

@@ -27,7 +27,7 @@ from vpd.case import FIELD, FIELD_WIDTH, VpdCase  # noqa: E402
 _D = ctypes.POINTER(ctypes.c_double)
 _I64 = ctypes.POINTER(ctypes.c_int64)
 _I32 = ctypes.POINTER(ctypes.c_int32)
-DIAG_COLS = 18
+DIAG_COLS = 20
 
 
 def _lib(name):

@@ -251,7 +251,8 @@ int vr_step(void *h, int32_t nsteps, double *diag) {
       const double sign = (c.bc_mode == VPD_BC_SMOOTH_DISPLACEMENT ? c.amplitude : c.grip_velocity) > 0 ? 1.0 : -1.0;
       double r[6];
       vo_ramp(&c, time, r);
-      double net[3] = {0, 0, 0}, reaction = 0, supportReaction = 0, avgS = 0, avgE = 0, maxEqps = 0, interior = 0;
+      double net[3] = {0, 0, 0}, reaction = 0, supportReaction = 0, avgS = 0, avgE = 0, maxEqps = 0, interior = 0,
+             plastic = 0;
       for (size_t i = 0; i < n; ++i) {
         for (int d = 0; d < 3; ++d)
           net[d] += s.force[i][d] * s.block.volume[i];
@@ -261,6 +262,8 @@ int vr_step(void *h, int32_t nsteps, double *diag) {
           interior += s.obsWeight[i];
         }
         maxEqps = std::max(maxEqps, s.mstate.vumatStateN[i][1]);
+        if (s.mstate.vumatStateN[i].size() > 4 && s.mstate.vumatStateN[i][4] > 0.0)
+          plastic += 1.0;
         for (int k = 0; k < 9; ++k)
           s.finite = s.finite && std::isfinite(result.rawStress[i][k]) && std::isfinite(result.strain[i][k]);
         for (int d = 0; d < 3; ++d)
@@ -313,6 +316,8 @@ int vr_step(void *h, int32_t nsteps, double *diag) {
         row[VPD_DIAG_ENERGY_ERROR] = energyError;
         row[VPD_DIAG_NET_INTERNAL_FORCE] = std::sqrt(net[0] * net[0] + net[1] * net[1] + net[2] * net[2]);
         row[VPD_DIAG_FINITE] = s.finite ? 1.0 : 0.0;
+        row[VPD_DIAG_PLASTIC_POINTS] = plastic;
+        row[VPD_DIAG_FALLBACK_POINTS] = 0.0;
       }
       s.damageIndex = damage.damageIndex;
       s.last = std::move(result);

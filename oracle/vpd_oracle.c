@@ -825,8 +825,10 @@ int vo_step(vo_sim *s, int32_t nsteps, double *diag) {
     double r[6];
     vo_ramp(c, time, r);
     double net[3] = {0, 0, 0}, reaction = 0.0, supportReaction = 0.0, avgS = 0.0, avgE = 0.0;
-    double maxEqps = 0.0, interior = 0.0;
+    double maxEqps = 0.0, interior = 0.0, plastic = 0.0;
     for (int64_t i = 0; i < n; ++i) {
+      if (c->nstatev > 4 && s->state[c->nstatev * i + 4] > 0.0)
+        plastic += 1.0;
       for (int d = 0; d < 3; ++d)
         net[d] += s->force[3 * i + d] * s->V[i];
       if (s->sets.obsWeight[i] > 0.0) {
@@ -896,6 +898,8 @@ int vo_step(vo_sim *s, int32_t nsteps, double *diag) {
       row[VPD_DIAG_ENERGY_ERROR] = energyError;
       row[VPD_DIAG_NET_INTERNAL_FORCE] = sqrt(net[0] * net[0] + net[1] * net[1] + net[2] * net[2]);
       row[VPD_DIAG_FINITE] = s->finite ? 1.0 : 0.0;
+      row[VPD_DIAG_PLASTIC_POINTS] = plastic;
+      row[VPD_DIAG_FALLBACK_POINTS] = 0.0;
     }
   }
   free(prevSig);

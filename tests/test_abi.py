@@ -34,19 +34,27 @@ def test_library_exports_every_declared_entry_point():
     assert lib.vpd_abi_version() == 1
 
 
-def test_case_struct_layout_matches_c():
-    fields = [f[0] for f in VpdCase._fields_]
+def c_layout(ctype: str, fields):
+    """sizeof and offsetof of a header struct, from a small C program."""
     prog = ["#include <stdio.h>", "#include <stddef.h>", f'#include "{HEADER}"', "int main(void){",
-            'printf("%zu\\n", sizeof(vpd_case));']
-    prog += [f'printf("%zu\\n", offsetof(vpd_case, {f}));' for f in fields]
+            f'printf("%zu\\n", sizeof({ctype}));']
+    prog += [f'printf("%zu\\n", offsetof({ctype}, {f}));' for f in fields]
     prog.append("return 0;}")
     with tempfile.TemporaryDirectory() as d:
         src, exe = os.path.join(d, "layout.c"), os.path.join(d, "layout")
         open(src, "w").write("\n".join(prog))
         subprocess.run(["gcc", src, "-o", exe], check=True)
-        out = [int(x) for x in subprocess.run([exe], capture_output=True, text=True).stdout.split()]
-    assert out[0] == ctypes.sizeof(VpdCase)
-    assert out[1:] == [getattr(VpdCase, f).offset for f in fields]
+        return [int(x) for x in subprocess.run([exe], capture_output=True, text=True).stdout.split()]
+
+
+@pytest.mark.parametrize("ctype,pytype", [("vpd_case", VpdCase),
+                                          ("vpd_surrogate_config", vpd.SurrogateConfig),
+                                          ("vpd_surrogate_report", vpd.SurrogateReport)])
+def test_struct_layouts_match_c(ctype, pytype):
+    fields = [f[0] for f in pytype._fields_]
+    out = c_layout(ctype, fields)
+    assert out[0] == ctypes.sizeof(pytype)
+    assert out[1:] == [getattr(pytype, f).offset for f in fields]
 
 
 def test_invalid_cases_rejected_on_host():

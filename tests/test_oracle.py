@@ -37,7 +37,8 @@ def test_oracle_matches_reference_library_fixture():
     bar = tensile_bar(1, jitter=0.05, jitter_seed=7, damage_mode=1, damage_initiation=0.004)
     sim = O.OracleSim(bar)
     diag = sim.step(300)
-    assert np.array_equal(diag, ref["diag"])
+    cols = ref["diag"].shape[1]  # the fixture predates the plastic/fallback columns
+    assert np.array_equal(diag[:, :cols], ref["diag"])
     assert np.array_equal(sim.get("displacement"), ref["displacement"])
     assert np.array_equal(sim.get("stress_corotational"), ref["stress_corotational"])
     assert np.array_equal(sim.get("state"), ref["state"])

@@ -230,6 +230,9 @@ struct vpd_handle {
   double *part_mat = nullptr, *part_force = nullptr, *accum = nullptr, *diag = nullptr;
   uint8_t *flags = nullptr;
   unsigned *status_dev = nullptr, *counter = nullptr;
+  uint16_t *surr_w = nullptr;  // surrogate network (device copies)
+  float *surr_b = nullptr;
+  bool surrogate_ready = false;
   StepParams params{};
 };
 
@@ -273,8 +276,8 @@ int check_case(const vpd_case *c) {
     return set_error(VPD_ERR_INVALID, "unknown damage mode");
   if (c->precision != VPD_PRECISION_FP64 && c->precision != VPD_PRECISION_MIXED)
     return set_error(VPD_ERR_INVALID, "unknown precision mode");
-  if (c->material_mode != VPD_MATERIAL_VUMAT)
-    return set_error(VPD_ERR_UNSUPPORTED, "this build implements the plain VUMAT material only");
+  if (c->material_mode != VPD_MATERIAL_VUMAT && c->material_mode != VPD_MATERIAL_SURROGATE)
+    return set_error(VPD_ERR_INVALID, "unknown material mode");
   for (int k = 0; k < 14; ++k)
     if (!std::isfinite(c->props[k]))
       return set_error(VPD_ERR_INVALID, "Johnson-Cook props must be finite");
@@ -291,6 +294,8 @@ int read_status(vpd_handle *h) {
     return set_error(VPD_ERR_SINGULAR, "Invalid deformation gradient determinant.");
   if (st & STATUS_SINGULAR_KINEMATICS)
     return set_error(VPD_ERR_SINGULAR, "Corotational update encountered a singular tensor.");
+  if (st & STATUS_SURROGATE_WAIT)
+    return set_error(VPD_ERR_CUDA, "surrogate material kernel: tensor-core wait timed out");
   return VPD_OK;
 }
 
@@ -430,6 +435,7 @@ int create_impl(vpd_handle *h, const vpd_case *c, const double *positions, const
   p.tension2 = (1.0 + c->damage_initiation) * (1.0 + c->damage_initiation);
   p.compression2 = c->damage_failure < 1.0 ? (1.0 - c->damage_failure) * (1.0 - c->damage_failure) : 0.0;
   p.tension2f = (float)p.tension2, p.compression2f = (float)p.compression2;
+  p.surrogate = c->material_mode == VPD_MATERIAL_SURROGATE;
   if (c->precision == VPD_PRECISION_MIXED) {
     if (!h->st.nw)
       return set_error(VPD_ERR_UNSUPPORTED,
@@ -581,6 +587,8 @@ int vpd_last_step_ms(const vpd_handle *h, double *ms) {
 int vpd_step(vpd_handle *h, int32_t nsteps, double *diag_out) {
   if (!h || nsteps < 0)
     return set_error(VPD_ERR_INVALID, "vpd_step needs a handle and nsteps >= 0");
+  if (h->params.surrogate && !h->surrogate_ready)
+    return set_error(VPD_ERR_INVALID, "material_mode is VPD_MATERIAL_SURROGATE: call vpd_set_surrogate first");
   if (nsteps == 0)
     return VPD_OK;
   int rc = ensure_graph(h);
@@ -607,6 +615,48 @@ int vpd_step(vpd_handle *h, int32_t nsteps, double *diag_out) {
   VPD_CUDA(cudaEventElapsedTime(&h->last_ms, h->ev0, h->ev1));
   h->step += nsteps;
   return read_status(h);
+}
+
+int vpd_set_surrogate(vpd_handle *h, const uint16_t *weights, const float *biases, int32_t guess,
+                      int32_t newton_steps) {
+  if (!h)
+    return set_error(VPD_ERR_INVALID, "vpd_set_surrogate: null handle");
+  if (!h->params.surrogate)
+    return set_error(VPD_ERR_INVALID, "vpd_set_surrogate: the case's material_mode is not VPD_MATERIAL_SURROGATE");
+  if (guess != VPD_GUESS_NETWORK && guess != VPD_GUESS_WARM_START && guess != VPD_GUESS_HYBRID)
+    return set_error(VPD_ERR_INVALID, "vpd_set_surrogate: unknown guess mode");
+  if (newton_steps < 0 || newton_steps > 50)
+    return set_error(VPD_ERR_INVALID, "vpd_set_surrogate: newton_steps must be in [0, 50]");
+  if (guess != VPD_GUESS_WARM_START && (!weights || !biases))
+    return set_error(VPD_ERR_INVALID, "vpd_set_surrogate: the network guess needs weights and biases");
+  if (guess != VPD_GUESS_WARM_START) {
+    for (int k = 0; k < VPD_MLP_PARAMS - VPD_MLP_WEIGHTS; ++k)
+      if (!std::isfinite(biases[k]))
+        return set_error(VPD_ERR_NONFINITE, "vpd_set_surrogate: non-finite bias");
+    int rc;
+    if (!h->surr_w && ((rc = dalloc(h, &h->surr_w, VPD_MLP_WEIGHTS)) ||
+                       (rc = dalloc(h, &h->surr_b, VPD_MLP_PARAMS - VPD_MLP_WEIGHTS))))
+      return rc;
+    VPD_CUDA(cudaMemcpyAsync(h->surr_w, weights, sizeof(uint16_t) * VPD_MLP_WEIGHTS, cudaMemcpyHostToDevice,
+                             h->stream));
+    VPD_CUDA(cudaMemcpyAsync(h->surr_b, biases, sizeof(float) * (VPD_MLP_PARAMS - VPD_MLP_WEIGHTS),
+                             cudaMemcpyHostToDevice, h->stream));
+    VPD_CUDA(cudaStreamSynchronize(h->stream));
+    int rc2 = prepare_material_surrogate();
+    if (rc2)
+      return rc2;
+  }
+  h->params.surr_guess = guess;
+  h->params.surr_steps = newton_steps;
+  h->params.sw = h->surr_w;
+  h->params.sb = h->surr_b;
+  h->surrogate_ready = true;
+  if (h->graph) {  // recaptured with the new parameters at the next vpd_step
+    VPD_CUDA(cudaStreamSynchronize(h->stream));
+    cudaGraphExecDestroy(h->graph);
+    h->graph = nullptr;
+  }
+  return VPD_OK;
 }
 
 int vpd_profile_increment(vpd_handle *h, int32_t nsteps, double *stage_ms) {

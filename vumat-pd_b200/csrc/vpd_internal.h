@@ -26,6 +26,7 @@ enum : unsigned int {
   STATUS_SINGULAR_K = 1u,
   STATUS_SINGULAR_F = 2u,
   STATUS_SINGULAR_KINEMATICS = 4u,
+  STATUS_SURROGATE_WAIT = 8u,  // a tensor-core wait of the surrogate material kernel timed out
 };
 
 // ---- point flags ----

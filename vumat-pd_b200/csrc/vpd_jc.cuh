@@ -49,49 +49,56 @@ struct JcPoint {
   double eInelastic;  // in/out
 };
 
-// One increment for one point. inc: strain increment (Voigt, tensor shear). Returns the
-// bisection iteration count (0 on the initialising call).
-__device__ __forceinline__ int jc_update(const JcParams &p, double dt, const double *inc,
-                                         JcPoint &pt) {
+// Elastic trial state of one increment (JohnsonCook.f90:74-112).
+struct JcTrial {
+  double trial[6], dev[6];
+  double pressure, qTrial, epOld, temperature, oldYield;
+};
+
+// Forms the trial state. On the first (initialising) call it completes the update of pt
+// itself and returns false.
+__device__ __forceinline__ bool jc_trial(const JcParams &p, const double *inc, JcPoint &pt, JcTrial &t) {
   const double traceInc = inc[0] + inc[1] + inc[2];
-  double trial[6];
 #pragma unroll
   for (int i = 0; i < 3; ++i)
-    trial[i] = pt.stress[i] + p.lambda * traceInc + 2.0 * p.mu * inc[i];
+    t.trial[i] = pt.stress[i] + p.lambda * traceInc + 2.0 * p.mu * inc[i];
 #pragma unroll
   for (int i = 3; i < 6; ++i)
-    trial[i] = pt.stress[i] + 2.0 * p.mu * inc[i];
+    t.trial[i] = pt.stress[i] + 2.0 * p.mu * inc[i];
 
   if (pt.state[0] == 0.0) {  // first call (:92-102)
     pt.state[0] = 1.0, pt.state[1] = 0.0, pt.state[2] = p.tref;
     pt.state[3] = 0.0, pt.state[4] = 0.0, pt.state[5] = 1.0;
 #pragma unroll
     for (int i = 0; i < 6; ++i)
-      pt.stress[i] = trial[i];
-    return 0;
+      pt.stress[i] = t.trial[i];
+    return false;
   }
-  const double epOld = pt.state[1], temperature = pt.state[2], oldYield = pt.state[3];
-  const double pressure = (trial[0] + trial[1] + trial[2]) / 3.0;
-  double dev[6];
+  t.epOld = pt.state[1], t.temperature = pt.state[2], t.oldYield = pt.state[3];
+  t.pressure = (t.trial[0] + t.trial[1] + t.trial[2]) / 3.0;
 #pragma unroll
   for (int i = 0; i < 3; ++i)
-    dev[i] = trial[i] - pressure;
+    t.dev[i] = t.trial[i] - t.pressure;
 #pragma unroll
   for (int i = 3; i < 6; ++i)
-    dev[i] = trial[i];
-  const double qTrial =
-      sqrt(1.5 * (dev[0] * dev[0] + dev[1] * dev[1] + dev[2] * dev[2] +
-                  2.0 * (dev[3] * dev[3] + dev[4] * dev[4] + dev[5] * dev[5])));
+    t.dev[i] = t.trial[i];
+  t.qTrial = sqrt(1.5 * (t.dev[0] * t.dev[0] + t.dev[1] * t.dev[1] + t.dev[2] * t.dev[2] +
+                         2.0 * (t.dev[3] * t.dev[3] + t.dev[4] * t.dev[4] + t.dev[5] * t.dev[5])));
+  return true;
+}
 
-  // Bracketed bisection with warm start (:114-136).
-  double epInc = 0.0, epLower = 0.0, epUpper = qTrial / (2.0 * p.mu), yield = oldYield;
+// Bracketed bisection with warm start (:114-136): plastic increment and yield stress; returns
+// the iteration count.
+__device__ __forceinline__ int jc_bisection(const JcParams &p, double dt, const JcTrial &t, double warmStart,
+                                            double &epIncOut, double &yieldOut) {
+  double epInc = 0.0, epLower = 0.0, epUpper = t.qTrial / (2.0 * p.mu), yield = t.oldYield;
   int iteration = 0;
   while (iteration < 50) {
     ++iteration;
     const double epRate = epInc / dt;
-    yield = jc_yield(p, epOld + epInc, epRate, temperature);
-    yield = yield > oldYield ? yield : oldYield;
-    double qNew = qTrial - 3.0 * p.mu * epInc;
+    yield = jc_yield(p, t.epOld + epInc, epRate, t.temperature);
+    yield = yield > t.oldYield ? yield : t.oldYield;
+    double qNew = t.qTrial - 3.0 * p.mu * epInc;
     qNew = qNew > 0.0 ? qNew : 0.0;
     const double residual = qNew - yield;
     if (fabs(residual) < p.tolerance)
@@ -104,27 +111,34 @@ __device__ __forceinline__ int jc_update(const JcParams &p, double dt, const dou
       epUpper = epUpper < epInc ? epUpper : epInc;
     epInc = 0.5 * (epLower + epUpper);
     if (iteration == 1) {
-      double warm = pt.state[4];
+      double warm = warmStart;
       warm = warm > epLower ? warm : epLower;
       epInc = warm < epUpper ? warm : epUpper;
     }
   }
+  epIncOut = epInc;
+  yieldOut = yield;
+  return iteration;
+}
 
+// Radial scaling, energies, heating and state for a given plastic increment (:138-156).
+__device__ __forceinline__ void jc_finish(const JcParams &p, const double *inc, const JcTrial &t, double epInc,
+                                          double yield, double iterations, JcPoint &pt) {
   double updated[6];
 #pragma unroll
   for (int i = 0; i < 6; ++i)
-    updated[i] = trial[i];
-  if (qTrial > 0.0) {  // radial scaling (:138-142)
-    double scale = 1.0 - 3.0 * p.mu * epInc / qTrial;
+    updated[i] = t.trial[i];
+  if (t.qTrial > 0.0) {  // radial scaling (:138-142)
+    double scale = 1.0 - 3.0 * p.mu * epInc / t.qTrial;
     scale = scale > 0.0 ? scale : 0.0;
 #pragma unroll
     for (int i = 0; i < 3; ++i)
-      updated[i] = pressure + scale * dev[i];
+      updated[i] = t.pressure + scale * t.dev[i];
 #pragma unroll
     for (int i = 3; i < 6; ++i)
-      updated[i] = scale * dev[i];
+      updated[i] = scale * t.dev[i];
   }
-  double qNew = qTrial - 3.0 * p.mu * epInc;
+  double qNew = t.qTrial - 3.0 * p.mu * epInc;
   qNew = qNew > 0.0 ? qNew : 0.0;
   double work = 0.0;
 #pragma unroll
@@ -138,11 +152,22 @@ __device__ __forceinline__ int jc_update(const JcParams &p, double dt, const dou
   pt.eInternal += workInc / p.rho;
   pt.eInelastic += plasticWork / p.rho;
   pt.state[0] = 1.0;
-  pt.state[1] = epOld + epInc;
-  pt.state[2] = temperature + p.workToHeat * p.beta * plasticWork / (p.rho * p.cp);
+  pt.state[1] = t.epOld + epInc;
+  pt.state[2] = t.temperature + p.workToHeat * p.beta * plasticWork / (p.rho * p.cp);
   pt.state[3] = yield;
   pt.state[4] = epInc;
-  pt.state[5] = pt.state[5] + (double)iteration;
+  pt.state[5] = pt.state[5] + iterations;
+}
+
+// One increment for one point. inc: strain increment (Voigt, tensor shear). Returns the
+// bisection iteration count (0 on the initialising call).
+__device__ __forceinline__ int jc_update(const JcParams &p, double dt, const double *inc, JcPoint &pt) {
+  JcTrial t;
+  if (!jc_trial(p, inc, pt, t))
+    return 0;
+  double epInc, yield;
+  const int iteration = jc_bisection(p, dt, t, pt.state[4], epInc, yield);
+  jc_finish(p, inc, t, epInc, yield, (double)iteration, pt);
   return iteration;
 }
 

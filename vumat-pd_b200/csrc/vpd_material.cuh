@@ -1,0 +1,205 @@
+// Per-point body of the material stage, shared by k_material (vpd_step.cu) and the surrogate
+// material kernel (vpd_surrogate.cu): F, the corotational update and the VUMAT's old state
+// (material_load); then, after the constitutive update, the spatial stress, the force map,
+// the history commit and the block's diagnostic partials (material_store).
+// VumatPdCorrespondenceMaterial::update (src/pd/VumatPdCorrespondenceMaterial.cpp:72-176) with
+// the kinematics of CorotationalKinematics.cpp:61-149.
+#pragma once
+
+#include "vpd_math.cuh"
+#include "vpd_step.cuh"
+
+namespace vpd {
+
+// Block-wide sums of K doubles; thread 0 writes them to out[slot * K].
+template <int K>
+__device__ __forceinline__ void block_partials(double (&v)[K], double *out, int64_t slot) {
+  __shared__ double red[32][K];
+#pragma unroll
+  for (int k = 0; k < K; ++k)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+      v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+      red[warp][k] = v[k];
+  __syncthreads();
+  if (threadIdx.x < K) {
+    double s = 0.0;
+    for (int w = 0; w < nw; ++w)
+      s += red[w][threadIdx.x];
+    out[(size_t)slot * K + threadIdx.x] = s;
+  }
+}
+
+// One point's material context between the kinematics and the stress update.
+struct MaterialPoint {
+  double F[9];      // deformation gradient of this increment
+  Corotational co;  // rotation, left stretch, unrotated rate of deformation
+  double E[6], Eold[6], oldFull[9];
+  double inc[6];    // corotational strain increment (Voigt, tensor shear)
+  JcPoint pt;       // VUMAT stress, state and energies (old on entry to the update)
+};
+
+__device__ __forceinline__ void material_load(const StepParams &p, int64_t i, MaterialPoint &m) {
+  const int64_t n = p.n;
+  double(&F)[9] = m.F;
+  Corotational &co = m.co;
+  double(&E)[6] = m.E;
+  double(&Eold)[6] = m.Eold;
+  double(&oldFull)[9] = m.oldFull;
+  JcPoint &pt = m.pt;
+  double Fn[9], Vn[9], Rn[9];
+  if (p.mixed) {  // F = I + G K^-1 in FP64 from the FP32 bond sum
+    double G[9], K[9];
+#pragma unroll
+    for (int c = 0; c < 9; ++c)
+      G[c] = (double)p.Gf[c * n + i], K[c] = p.kinv[c * n + i];
+    m_mul(G, K, F);
+#pragma unroll
+    for (int c = 0; c < 9; c += 4)
+      F[c] += 1.0;
+  } else {
+#pragma unroll
+    for (int c = 0; c < 9; ++c)
+      F[c] = p.F[c * n + i];
+  }
+#pragma unroll
+  for (int c = 0; c < 9; ++c) {
+    Fn[c] = p.Fn[c * n + i];
+    Vn[c] = p.Vn[c * n + i];
+    Rn[c] = p.Rn[c * n + i];
+  }
+  if (!corotational_update(Fn, F, Vn, Rn, p.dt, co)) {
+    atomicOr(p.status, STATUS_SINGULAR_KINEMATICS);
+#pragma unroll
+    for (int c = 0; c < 9; ++c)
+      co.dbar[c] = 0.0, co.spin[c] = 0.0, co.r[c] = Rn[c], co.v[c] = Vn[c];
+  }
+  green_lagrange6(F, E);
+#pragma unroll
+  for (int c = 0; c < 6; ++c) {
+    Eold[c] = p.En[c * n + i];
+    pt.stress[c] = p.sig[c * n + i];
+    pt.state[c] = p.state[c * n + i];
+  }
+  pt.eInternal = p.eI[i];
+  pt.eInelastic = p.eP[i];
+  voigt_to_full(pt.stress, oldFull);
+  const double *d = co.dbar;
+  m.inc[0] = d[0] * p.dt, m.inc[1] = d[4] * p.dt, m.inc[2] = d[8] * p.dt;
+  m.inc[3] = 0.5 * (d[5] + d[7]) * p.dt, m.inc[4] = 0.5 * (d[2] + d[6]) * p.dt;
+  m.inc[5] = 0.5 * (d[1] + d[3]) * p.dt;
+}
+
+// part[PM_*] and maxEqps receive this point's diagnostic contributions.
+__device__ __forceinline__ void material_store(const StepParams &p, int64_t i, MaterialPoint &m, double *part,
+                                               double &maxEqps) {
+  const int64_t n = p.n;
+  const double(&F)[9] = m.F;
+  const Corotational &co = m.co;
+  const double(&E)[6] = m.E;
+  const double(&Eold)[6] = m.Eold;
+  const double(&oldFull)[9] = m.oldFull;
+  const JcPoint &pt = m.pt;
+  double full[9], spatial[9], K[9], M[9];
+  voigt_to_full(pt.stress, full);
+  rotate_to_spatial(full, co.r, spatial);
+#pragma unroll
+  for (int c = 0; c < 9; ++c)
+    K[c] = p.kinv[c * n + i];
+  if (!force_map(spatial, F, K, M)) {
+    atomicOr(p.status, STATUS_SINGULAR_F);
+#pragma unroll
+    for (int c = 0; c < 9; ++c)
+      M[c] = 0.0;
+  }
+#pragma unroll
+  for (int c = 0; c < 9; ++c) {
+    p.Fn[c * n + i] = F[c];
+    p.Vn[c * n + i] = co.v[c];
+    p.Rn[c * n + i] = co.r[c];
+  }
+  // the force map scaled by the point's volume, in the layout the force kernel gathers
+  const double4 xi = p.xv[i];
+  const double vol = xi.w;
+  if (p.mixed) {
+    const float4 ji = p.jit[i];
+    const float jr[3] = {ji.x, ji.y, ji.z};
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+      p.fmapf[r * n + i] = make_float4((float)(vol * M[3 * r]), (float)(vol * M[3 * r + 1]),
+                                       (float)(vol * M[3 * r + 2]), jr[r]);
+  } else if (p.fmap) {
+    const double xr[3] = {xi.x, xi.y, xi.z};
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+      st256(p.fmap + r * n + i, make_double4(vol * M[3 * r], vol * M[3 * r + 1], vol * M[3 * r + 2], xr[r]));
+  } else {
+    double2 *Mt = reinterpret_cast<double2 *>(p.Mt + 10 * i);
+    Mt[0] = make_double2(vol * M[0], vol * M[1]);
+    Mt[1] = make_double2(vol * M[2], vol * M[3]);
+    Mt[2] = make_double2(vol * M[4], vol * M[5]);
+    Mt[3] = make_double2(vol * M[6], vol * M[7]);
+    Mt[4] = make_double2(vol * M[8], 0.0);
+  }
+#pragma unroll
+  for (int c = 0; c < 6; ++c) {
+    p.En[c * n + i] = E[c];
+    p.sig[c * n + i] = pt.stress[c];
+    p.state[c * n + i] = pt.state[c];
+  }
+  p.eI[i] = pt.eInternal;
+  p.eP[i] = pt.eInelastic;
+  // diagnostics: internal-energy increment with the reference's mixed-frame average
+  // (BoundaryValueCaseRunner.cpp:231-238), observation-window means, max eqps, finiteness
+  const double a0 = 0.5 * (oldFull[0] + spatial[0]), a4 = 0.5 * (oldFull[4] + spatial[4]);
+  const double a8 = 0.5 * (oldFull[8] + spatial[8]), a1 = 0.5 * (oldFull[1] + spatial[1]);
+  const double a2 = 0.5 * (oldFull[2] + spatial[2]), a5 = 0.5 * (oldFull[5] + spatial[5]);
+  const double e11 = E[0] - Eold[0], e22 = E[1] - Eold[1], e33 = E[2] - Eold[2];
+  const double e23 = E[3] - Eold[3], e13 = E[4] - Eold[4], e12 = E[5] - Eold[5];
+  part[PM_DU] = (a0 * e11 + a4 * e22 + a8 * e33 + 2.0 * (a1 * e12 + a2 * e13 + a5 * e23)) * vol;
+  const double w = p.obsw[i];
+  if (w > 0.0) {
+    // selects rather than a runtime index, which would put the arrays in local memory
+    const int ax = p.bc.axis;
+    const double sa = ax == 0 ? spatial[0] : (ax == 1 ? spatial[4] : spatial[8]);
+    const double ea = ax == 0 ? E[0] : (ax == 1 ? E[1] : E[2]);
+    part[PM_AVG_STRESS] = p.sign * sa * w;
+    part[PM_AVG_STRAIN] = p.sign * ea * w;
+  }
+  maxEqps = pt.state[1];
+  bool fin = true;
+#pragma unroll
+  for (int c = 0; c < 9; ++c)
+    fin = fin && isfinite(spatial[c]);
+#pragma unroll
+  for (int c = 0; c < 6; ++c)
+    fin = fin && isfinite(E[c]) && isfinite(pt.state[c]);
+  part[PM_NONFINITE] = fin ? 0.0 : 1.0;
+  part[PM_PLASTIC] = pt.state[4] > 0.0 ? 1.0 : 0.0;
+}
+
+// Reduces the block's partials of one 128-point tile into p.part_mat[slot] (sums; max for
+// PM_MAX_EQPS). Every thread of the block calls it (it contains __syncthreads).
+__device__ __forceinline__ void material_reduce(const StepParams &p, double (&part)[PM_COUNT], double maxEqps,
+                                                int64_t slot) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1)
+    maxEqps = fmax(maxEqps, __shfl_xor_sync(0xffffffffu, maxEqps, o));
+  __shared__ double smax[32];
+  if ((threadIdx.x & 31) == 0)
+    smax[threadIdx.x >> 5] = maxEqps;
+  block_partials<PM_COUNT>(part, p.part_mat, slot);  // contains __syncthreads
+  if (threadIdx.x == 0) {
+    double m = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w)
+      m = fmax(m, smax[w]);
+    p.part_mat[(size_t)slot * PM_COUNT + PM_MAX_EQPS] = m;
+  }
+  __syncthreads();  // smax and block_partials' buffer are reused by the next tile
+}
+
+}  // namespace vpd

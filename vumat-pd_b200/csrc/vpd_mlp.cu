@@ -11,79 +11,12 @@
 // Backward (same tiling): dZ = dY * SiLU'(Z); dW = dZ^T Y_prev is a 128 x 128 (or 128 x 16)
 // product over the tile's rows, accumulated into FP32 gradient buffers with atomics; dY_prev =
 // dZ W. Operands that the products need transposed are staged transposed into shared memory.
-#include "vpd_mlp.cuh"
-#include "vpd_umma.cuh"
+#include "vpd_mlp_tile.cuh"
 
 #include <algorithm>
 #include <vector>
 
 namespace vpd {
-
-using umma::kmajor_offset;
-using umma::smem_u32;
-
-constexpr uint32_t kWaitLimit = 1u << 24;  // mbarrier polls before a wait is declared failed
-
-__device__ __forceinline__ float silu(float z) { return z / (1.0f + __expf(-z)); }
-__device__ __forceinline__ float silu_grad(float z) {
-  const float s = 1.0f / (1.0f + __expf(-z));
-  return s * (1.0f + z * (1.0f - s));
-}
-
-// Shared-memory store of one bf16 element at (row, k) of a K-major tile.
-__device__ __forceinline__ void st_bf16(unsigned char *tile, int row, int k, int ktotal, float v) {
-  *reinterpret_cast<__nv_bfloat16 *>(tile + kmajor_offset(row, k, ktotal)) = __float2bfloat16(v);
-}
-
-// Copies a row-major bf16 matrix [rows][cols] into a K-major tile (K = cols), 16 bytes at a time.
-__device__ __forceinline__ void stage_rowmajor(unsigned char *tile, const __nv_bfloat16 *src, int rows, int cols) {
-  const int chunks = rows * cols / 8;
-  for (int c = threadIdx.x; c < chunks; c += blockDim.x) {
-    const int row = c / (cols / 8), k = (c % (cols / 8)) * 8;
-    *reinterpret_cast<uint4 *>(tile + kmajor_offset(row, k, cols)) =
-        *reinterpret_cast<const uint4 *>(src + (size_t)row * cols + k);
-  }
-}
-
-// Copies the transpose of a row-major bf16 matrix [rows][cols] into a K-major tile whose rows
-// are the source columns (K = rows).
-__device__ __forceinline__ void stage_transposed(unsigned char *tile, const __nv_bfloat16 *src, int rows, int cols) {
-  for (int e = threadIdx.x; e < rows * cols; e += blockDim.x) {
-    const int r = e / cols, c = e % cols;
-    *reinterpret_cast<__nv_bfloat16 *>(tile + kmajor_offset(c, r, rows)) = src[(size_t)r * cols + c];
-  }
-}
-
-struct Sync {
-  uint64_t *mbar;
-  uint32_t phase;
-  unsigned *err;
-  bool ok;
-  // Every thread of the block calls this; the outcome is made uniform so a timeout cannot
-  // split the block's control flow around later barriers.
-  __device__ void wait() {
-    const bool got = ok && umma::mbar_wait(mbar, phase, kWaitLimit);
-    ok = __syncthreads_and(got) != 0;
-    if (!ok && threadIdx.x == 0)
-      atomicOr(err, 1u);
-    phase ^= 1u;
-    umma::fence_after_sync();
-  }
-};
-
-// Issues D = A * B^T on one thread and waits for it on all threads.
-__device__ __forceinline__ void gemm(Sync &sy, uint32_t tmem_d, const unsigned char *a, const unsigned char *b,
-                                     int K, int N) {
-  umma::fence_proxy_async();
-  umma::fence_before_sync();
-  __syncthreads();
-  umma::fence_after_sync();
-  if (threadIdx.x == 0) {
-    umma::gemm_issue(tmem_d, smem_u32(a), smem_u32(b), K, N, false);
-    umma::commit(sy.mbar);
-  }
-  sy.wait();
-}
 
 // ------------------------------------------------------------------ forward
 // smem: W1 (128x16) | W2 (128x128) | W3 | W4 (16x128) | A (128x128) | X0 (128x16) | barrier
@@ -94,33 +27,6 @@ __device__ __forceinline__ void stage_weights_fwd(unsigned char *s, const MlpWei
   stage_rowmajor(s + 4096, w.w2, kMlpHidden, kMlpHidden);
   stage_rowmajor(s + 4096 + 32768, w.w3, kMlpHidden, kMlpHidden);
   stage_rowmajor(s + 4096 + 65536, w.w4, kMlpOut, kMlpHidden);
-}
-
-// Hidden-layer epilogue for the calling thread's row: bias, SiLU, next operand (bf16) in A;
-// optionally the pre-activation and activation to global memory.
-__device__ __forceinline__ void hidden_epilogue(uint32_t trow, const float *bias, unsigned char *A, float *z_out,
-                                                __nv_bfloat16 *y_out) {
-  const int t = threadIdx.x;
-  for (int c0 = 0; c0 < kMlpHidden; c0 += 16) {
-    float v[16];
-    umma::tmem_ld16(trow + c0, v);
-    __align__(16) __nv_bfloat16 yb[16];
-#pragma unroll
-    for (int c = 0; c < 16; ++c) {
-      const float z = v[c] + bias[c0 + c];
-      yb[c] = __float2bfloat16(silu(z));
-      if (z_out)
-        z_out[c0 + c] = z;
-    }
-    // two 16-byte rows of core matrices
-    *reinterpret_cast<uint4 *>(A + kmajor_offset(t, c0, kMlpHidden)) = *reinterpret_cast<const uint4 *>(yb);
-    *reinterpret_cast<uint4 *>(A + kmajor_offset(t, c0 + 8, kMlpHidden)) =
-        *reinterpret_cast<const uint4 *>(yb + 8);
-    if (y_out) {
-      *reinterpret_cast<uint4 *>(y_out + c0) = *reinterpret_cast<const uint4 *>(yb);
-      *reinterpret_cast<uint4 *>(y_out + c0 + 8) = *reinterpret_cast<const uint4 *>(yb + 8);
-    }
-  }
 }
 
 __global__ void __launch_bounds__(128, 1) k_mlp_forward(MlpWeights w, const float *x, int64_t B, float *out,
@@ -153,7 +59,7 @@ __global__ void __launch_bounds__(128, 1) k_mlp_forward(MlpWeights w, const floa
   umma::fence_after_sync();
   const uint32_t tmem = s_tmem;
   const uint32_t trow = tmem + ((uint32_t)(t & ~31) << 16);  // this warp's TMEM lanes
-  Sync sy{mbar, 0u, err, true};
+  Sync sy{mbar, 0u, err, 1u, true};
   const bool keep = row < B;
   gemm(sy, tmem, sX, sW1, kMlpIn, kMlpHidden);
   hidden_epilogue(trow, w.b1, sA, keep && acts.z1 ? acts.z1 + row * kMlpHidden : nullptr,
@@ -220,7 +126,7 @@ __global__ void __launch_bounds__(128, 1) k_mlp_backward(MlpWeights w, MlpActs a
   const uint32_t tmem = s_tmem;
   const uint32_t lane_base = (uint32_t)(t & ~31) << 16;
   const uint32_t tdy = tmem + lane_base, tdw = tmem + 128 + lane_base;
-  Sync sy{mbar, 0u, err, true};
+  Sync sy{mbar, 0u, err, 1u, true};
 
   // ---- output layer: dZ4 = gout
   float dz4[kMlpOut];

@@ -33,11 +33,11 @@ struct MlpGrads {  // FP32 accumulators, same shapes as the parameters
   float *w1, *w2, *w3, *w4, *b1, *b2, *b3, *b4;
 };
 
-inline MlpWeights mlp_weights(const __nv_bfloat16 *wb, const float *bias) {
+__host__ __device__ inline MlpWeights mlp_weights(const __nv_bfloat16 *wb, const float *bias) {
   return MlpWeights{wb, wb + 2048, wb + 2048 + 16384, wb + 2048 + 32768,
                     bias, bias + 128, bias + 256, bias + 384};
 }
-inline MlpGrads mlp_grads(float *g) {
+__host__ __device__ inline MlpGrads mlp_grads(float *g) {
   return MlpGrads{g, g + 2048, g + 2048 + 16384, g + 2048 + 32768,
                   g + kMlpWeights, g + kMlpWeights + 128, g + kMlpWeights + 256, g + kMlpWeights + 384};
 }

@@ -19,6 +19,7 @@
 // deterministically: each block writes a partial, the last block of k_integrate sums them in
 // block order and writes the increment's row.
 #include "vpd_math.cuh"
+#include "vpd_material.cuh"
 #include "vpd_step.cuh"
 
 namespace vpd {
@@ -83,29 +84,6 @@ __device__ __forceinline__ void apply_bc(const BcParams &b, uint8_t fl, const do
     u.z = 0.0, v.z = 0.0, a.z = 0.0;
   if (b.plane_strain)
     u.z = 0.0, v.z = 0.0, a.z = 0.0;
-}
-
-// Block-wide sums of K doubles; thread 0 of each block writes them to out[blockIdx.x * K].
-template <int K>
-__device__ __forceinline__ void block_partials(double (&v)[K], double *out) {
-  __shared__ double red[32][K];
-#pragma unroll
-  for (int k = 0; k < K; ++k)
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1)
-      v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  if (lane == 0)
-#pragma unroll
-    for (int k = 0; k < K; ++k)
-      red[warp][k] = v[k];
-  __syncthreads();
-  if (threadIdx.x < K) {
-    double s = 0.0;
-    for (int w = 0; w < nw; ++w)
-      s += red[w][threadIdx.x];
-    out[(size_t)blockIdx.x * K + threadIdx.x] = s;
-  }
 }
 
 // ------------------------------------------------------------------ k_deformation
@@ -197,143 +175,17 @@ __global__ void __launch_bounds__(kBondThreads) k_deformation(StepParams p) {
 }
 
 // ------------------------------------------------------------------ k_material
-__global__ void __launch_bounds__(kMaterialThreads) k_material(StepParams p) {
-  const int64_t n = p.n;
+__global__ void __launch_bounds__(kMaterialThreads) k_material(const __grid_constant__ StepParams p) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  double part[PM_COUNT] = {0, 0, 0, 0, 0};
+  double part[PM_COUNT] = {};
   double maxEqps = 0.0;
-  if (i < n) {
-    double F[9], Fn[9], Vn[9], Rn[9];
-    if (p.mixed) {  // F = I + G K^-1 in FP64 from the FP32 bond sum
-      double G[9], K[9];
-#pragma unroll
-      for (int c = 0; c < 9; ++c)
-        G[c] = (double)p.Gf[c * n + i], K[c] = p.kinv[c * n + i];
-      m_mul(G, K, F);
-#pragma unroll
-      for (int c = 0; c < 9; c += 4)
-        F[c] += 1.0;
-    } else {
-#pragma unroll
-      for (int c = 0; c < 9; ++c)
-        F[c] = p.F[c * n + i];
-    }
-#pragma unroll
-    for (int c = 0; c < 9; ++c) {
-      Fn[c] = p.Fn[c * n + i];
-      Vn[c] = p.Vn[c * n + i];
-      Rn[c] = p.Rn[c * n + i];
-    }
-    Corotational co;
-    if (!corotational_update(Fn, F, Vn, Rn, p.dt, co)) {
-      atomicOr(p.status, STATUS_SINGULAR_KINEMATICS);
-#pragma unroll
-      for (int c = 0; c < 9; ++c)
-        co.dbar[c] = 0.0, co.spin[c] = 0.0, co.r[c] = Rn[c], co.v[c] = Vn[c];
-    }
-    double E[6], Eold[6];
-    green_lagrange6(F, E);
-    JcPoint pt;
-#pragma unroll
-    for (int c = 0; c < 6; ++c) {
-      Eold[c] = p.En[c * n + i];
-      pt.stress[c] = p.sig[c * n + i];
-      pt.state[c] = p.state[c * n + i];
-    }
-    pt.eInternal = p.eI[i];
-    pt.eInelastic = p.eP[i];
-    double oldFull[9];
-    voigt_to_full(pt.stress, oldFull);
-    const double *d = co.dbar;
-    const double inc[6] = {d[0] * p.dt, d[4] * p.dt, d[8] * p.dt, 0.5 * (d[5] + d[7]) * p.dt,
-                           0.5 * (d[2] + d[6]) * p.dt, 0.5 * (d[1] + d[3]) * p.dt};
-    jc_update(p.jc, p.dt, inc, pt);
-    double full[9], spatial[9], K[9], M[9];
-    voigt_to_full(pt.stress, full);
-    rotate_to_spatial(full, co.r, spatial);
-#pragma unroll
-    for (int c = 0; c < 9; ++c)
-      K[c] = p.kinv[c * n + i];
-    if (!force_map(spatial, F, K, M)) {
-      atomicOr(p.status, STATUS_SINGULAR_F);
-#pragma unroll
-      for (int c = 0; c < 9; ++c)
-        M[c] = 0.0;
-    }
-#pragma unroll
-    for (int c = 0; c < 9; ++c) {
-      p.Fn[c * n + i] = F[c];
-      p.Vn[c * n + i] = co.v[c];
-      p.Rn[c * n + i] = co.r[c];
-    }
-    // the force map scaled by the point's volume, in the layout the force kernel gathers
-    const double4 xi = p.xv[i];
-    const double vol = xi.w;
-    if (p.mixed) {
-      const float4 ji = p.jit[i];
-      const float jr[3] = {ji.x, ji.y, ji.z};
-#pragma unroll
-      for (int r = 0; r < 3; ++r)
-        p.fmapf[r * n + i] = make_float4((float)(vol * M[3 * r]), (float)(vol * M[3 * r + 1]),
-                                         (float)(vol * M[3 * r + 2]), jr[r]);
-    } else if (p.fmap) {
-      const double xr[3] = {xi.x, xi.y, xi.z};
-#pragma unroll
-      for (int r = 0; r < 3; ++r)
-        st256(p.fmap + r * n + i, make_double4(vol * M[3 * r], vol * M[3 * r + 1], vol * M[3 * r + 2], xr[r]));
-    } else {
-      double2 *Mt = reinterpret_cast<double2 *>(p.Mt + 10 * i);
-      Mt[0] = make_double2(vol * M[0], vol * M[1]);
-      Mt[1] = make_double2(vol * M[2], vol * M[3]);
-      Mt[2] = make_double2(vol * M[4], vol * M[5]);
-      Mt[3] = make_double2(vol * M[6], vol * M[7]);
-      Mt[4] = make_double2(vol * M[8], 0.0);
-    }
-#pragma unroll
-    for (int c = 0; c < 6; ++c) {
-      p.En[c * n + i] = E[c];
-      p.sig[c * n + i] = pt.stress[c];
-      p.state[c * n + i] = pt.state[c];
-    }
-    p.eI[i] = pt.eInternal;
-    p.eP[i] = pt.eInelastic;
-    // diagnostics: internal-energy increment with the reference's mixed-frame average
-    // (BoundaryValueCaseRunner.cpp:231-238), observation-window means, max eqps, finiteness
-    const double a0 = 0.5 * (oldFull[0] + spatial[0]), a4 = 0.5 * (oldFull[4] + spatial[4]);
-    const double a8 = 0.5 * (oldFull[8] + spatial[8]), a1 = 0.5 * (oldFull[1] + spatial[1]);
-    const double a2 = 0.5 * (oldFull[2] + spatial[2]), a5 = 0.5 * (oldFull[5] + spatial[5]);
-    const double e11 = E[0] - Eold[0], e22 = E[1] - Eold[1], e33 = E[2] - Eold[2];
-    const double e23 = E[3] - Eold[3], e13 = E[4] - Eold[4], e12 = E[5] - Eold[5];
-    part[PM_DU] = (a0 * e11 + a4 * e22 + a8 * e33 + 2.0 * (a1 * e12 + a2 * e13 + a5 * e23)) * vol;
-    const double w = p.obsw[i];
-    if (w > 0.0) {
-      part[PM_AVG_STRESS] = p.sign * spatial[4 * p.bc.axis] * w;
-      part[PM_AVG_STRAIN] = p.sign * E[p.bc.axis] * w;
-    }
-    maxEqps = pt.state[1];
-    bool fin = true;
-#pragma unroll
-    for (int c = 0; c < 9; ++c)
-      fin = fin && isfinite(spatial[c]);
-#pragma unroll
-    for (int c = 0; c < 6; ++c)
-      fin = fin && isfinite(E[c]) && isfinite(pt.state[c]);
-    part[PM_NONFINITE] = fin ? 0.0 : 1.0;
+  if (i < p.n) {
+    MaterialPoint m;
+    material_load(p, i, m);
+    jc_update(p.jc, p.dt, m.inc, m.pt);
+    material_store(p, i, m, part, maxEqps);
   }
-  // max over the block for eqps, sums for the rest
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1)
-    maxEqps = fmax(maxEqps, __shfl_xor_sync(0xffffffffu, maxEqps, o));
-  __shared__ double smax[32];
-  if ((threadIdx.x & 31) == 0)
-    smax[threadIdx.x >> 5] = maxEqps;
-  block_partials<PM_COUNT>(part, p.part_mat);  // contains __syncthreads
-  if (threadIdx.x == 0) {
-    double m = 0.0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w)
-      m = fmax(m, smax[w]);
-    p.part_mat[(size_t)blockIdx.x * PM_COUNT + PM_MAX_EQPS] = m;
-  }
+  material_reduce(p, part, maxEqps, blockIdx.x);
 }
 
 // ------------------------------------------------------------------ k_force (sliced ELL)
@@ -438,7 +290,7 @@ __global__ void __launch_bounds__(kBondThreads) k_integrate(StepParams p) {
     if (p.mixed)
       p.uf[i] = make_float4((float)un.x, (float)un.y, (float)un.z, 0.0f);
   }
-  block_partials<PF_COUNT>(part, p.part_force);
+  block_partials<PF_COUNT>(part, p.part_force, blockIdx.x);
 
   // last block: reduce every block's partials in block order and write the diagnostic row
   __shared__ bool last;
@@ -530,6 +382,8 @@ __global__ void __launch_bounds__(kBondThreads) k_integrate(StepParams p) {
   row[VPD_DIAG_NET_INTERNAL_FORCE] =
       sqrt(pf[PF_NETX] * pf[PF_NETX] + pf[PF_NETY] * pf[PF_NETY] + pf[PF_NETZ] * pf[PF_NETZ]);
   row[VPD_DIAG_FINITE] = finite ? 1.0 : 0.0;
+  row[VPD_DIAG_PLASTIC_POINTS] = pm[PM_PLASTIC];
+  row[VPD_DIAG_FALLBACK_POINTS] = pm[PM_FALLBACK];
   *p.counter = 0u;
   *p.step = step + 1;
 }
@@ -640,6 +494,8 @@ int launch_stage(int stage, const StepParams &p, cudaStream_t s) {
       return launch_deformation_stencil(p, s);
     k_deformation<<<bond_grid(p.n), kBondThreads, 0, s>>>(p);
   } else if (stage == 1) {
+    if (p.surrogate)
+      return launch_material_surrogate(p, s);
     k_material<<<(unsigned)material_grid(p.n), kMaterialThreads, 0, s>>>(p);
   } else if (stage == 2) {
     if (p.mixed)

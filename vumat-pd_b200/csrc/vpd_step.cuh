@@ -12,7 +12,7 @@ struct BcParams {
 };
 
 // Quantities each material block reduces (sums except the max).
-enum { PM_DU = 0, PM_AVG_STRESS, PM_AVG_STRAIN, PM_MAX_EQPS, PM_NONFINITE, PM_COUNT };
+enum { PM_DU = 0, PM_AVG_STRESS, PM_AVG_STRAIN, PM_MAX_EQPS, PM_NONFINITE, PM_PLASTIC, PM_FALLBACK, PM_COUNT };
 // Quantities each force block reduces (sums).
 enum {
   PF_NETX = 0, PF_NETY, PF_NETZ, PF_REACTION, PF_SUPPORT_REACTION, PF_KINETIC, PF_LAT_POS,
@@ -65,6 +65,12 @@ struct StepParams {
   float *Gf;                  // sum V_j (u_j - u_i) (x) xi, 9 floats structure of arrays
   float4 *fmapf;              // fmapf[r * n + i] = (VM_r0, VM_r1, VM_r2, jit_r) in FP32
   float tension2f, compression2f;
+  // surrogate material update (VPD_MATERIAL_SURROGATE, vpd_surrogate.cu)
+  int surrogate;              // 1: guess + Newton, bisection fallback, instead of the bisection
+  int surr_guess;             // VPD_GUESS_*: the network, or the previous plastic increment
+  int surr_steps;             // Newton steps allowed after the guess
+  const uint16_t *sw;         // network weights (bf16 bits, VPD_MLP_WEIGHTS)
+  const float *sb;            // network biases (400)
   int nstatev;
   // boundary and diagnostics sets
   const uint8_t *flags;
@@ -103,6 +109,9 @@ int launch_shape_stencil(const StepParams &p, cudaStream_t s);
 int launch_deformation_stencil(const StepParams &p, cudaStream_t s);
 int launch_force_stencil(const StepParams &p, cudaStream_t s);
 int launch_damage_index_stencil(const StepParams &p, double *out, cudaStream_t s);
+// surrogate material update (vpd_surrogate.cu)
+int launch_material_surrogate(const StepParams &p, cudaStream_t s);
+int prepare_material_surrogate();  // kernel attributes; call before any capture
 // mixed precision (vpd_mixed.cu)
 int launch_deformation_mixed(const StepParams &p, cudaStream_t s);
 int launch_force_mixed(const StepParams &p, cudaStream_t s);

@@ -89,6 +89,10 @@ def library():
     lib.vpd_damage_update.argtypes = [_VP, _VP, _VP, ctypes.c_int64, _VP, _VP, ctypes.c_double,
                                       ctypes.c_double, _VP, _VP, _VP]
     lib.vpd_mlp_forward.argtypes = [_VP, _VP, _VP, ctypes.c_int64, _VP, _VP]
+    lib.vpd_surrogate_samples.argtypes = [_D, ctypes.c_uint64, ctypes.c_int64, _VP, _VP, _VP]
+    lib.vpd_train_surrogate.argtypes = [ctypes.POINTER(SurrogateConfig), _VP, _VP,
+                                        ctypes.POINTER(SurrogateReport)]
+    lib.vpd_set_surrogate.argtypes = [_VP, _VP, _VP, ctypes.c_int32, ctypes.c_int32]
     lib.vpd_mlp_gradients.argtypes = [_VP, _VP, _VP, _VP, ctypes.c_int64, _VP, _VP]
     _lib = lib
     return lib
@@ -101,6 +105,59 @@ def _check(rc: int):
 
 def _dp(a: np.ndarray):
     return a.ctypes.data_as(_D)
+
+
+MAX_EPOCHS = 64
+SAMPLE_RECORD = 26
+GUESS = {"network": 0, "warm_start": 1, "hybrid": 2}
+
+
+class SurrogateConfig(ctypes.Structure):
+    _fields_ = [("props", ctypes.c_double * 14), ("samples", ctypes.c_int64),
+                ("epochs", ctypes.c_int32), ("batch", ctypes.c_int32),
+                ("learning_rate", ctypes.c_double), ("seed", ctypes.c_uint64),
+                ("validation_fraction", ctypes.c_double)]
+
+
+class SurrogateReport(ctypes.Structure):
+    _fields_ = [("epochs_run", ctypes.c_int32), ("epoch_loss", ctypes.c_double * MAX_EPOCHS),
+                ("validation_loss", ctypes.c_double), ("ratio_rmse", ctypes.c_double),
+                ("stress_rmse", ctypes.c_double), ("plastic_fraction", ctypes.c_double),
+                ("train_ms", ctypes.c_double)]
+
+
+def surrogate_samples(props, seed: int, count: int, records: bool = False):
+    """Increments solved by the device VUMAT: (features [count,16], targets [count,16],
+    records [count, SAMPLE_RECORD] or None), float32 / float64 numpy arrays."""
+    props = np.ascontiguousarray(props, dtype=np.float64)
+    f = np.zeros((count, 16), dtype=np.float32)
+    t = np.zeros((count, 16), dtype=np.float32)
+    r = np.zeros((count, SAMPLE_RECORD)) if records else None
+    _check(library().vpd_surrogate_samples(_dp(props), seed, count, f.ctypes.data_as(_VP),
+                                           t.ctypes.data_as(_VP),
+                                           None if r is None else r.ctypes.data_as(_VP)))
+    return f, t, r
+
+
+def train_surrogate(props, samples: int = 2_000_000, epochs: int = 20, batch: int = 8192,
+                    learning_rate: float = 1e-3, seed: int = 2026, validation_fraction: float = 0.05):
+    """Trains the Johnson-Cook surrogate on the GPU. Returns (weights uint16 [VPD_MLP_WEIGHTS],
+    biases float32 [400], report dict)."""
+    cfg = SurrogateConfig()
+    for k, v in enumerate(props):
+        cfg.props[k] = float(v)
+    cfg.samples, cfg.epochs, cfg.batch = samples, epochs, batch
+    cfg.learning_rate, cfg.seed, cfg.validation_fraction = learning_rate, seed, validation_fraction
+    w = np.zeros(MLP_WEIGHTS, dtype=np.uint16)
+    b = np.zeros(MLP_PARAMS - MLP_WEIGHTS, dtype=np.float32)
+    rep = SurrogateReport()
+    _check(library().vpd_train_surrogate(ctypes.byref(cfg), w.ctypes.data_as(_VP),
+                                         b.ctypes.data_as(_VP), ctypes.byref(rep)))
+    report = {"epoch_loss": [rep.epoch_loss[e] for e in range(rep.epochs_run)],
+              "validation_loss": rep.validation_loss, "ratio_rmse": rep.ratio_rmse,
+              "stress_rmse": rep.stress_rmse, "plastic_fraction": rep.plastic_fraction,
+              "train_ms": rep.train_ms}
+    return w, b, report
 
 
 class Simulation:
@@ -131,10 +188,19 @@ class Simulation:
         return int(library().vpd_bond_layout_words(self._h))
 
     def step(self, nsteps: int, diagnostics: bool = True) -> np.ndarray | None:
-        """Advances nsteps increments; returns nsteps x 18 timeseries rows."""
+        """Advances nsteps increments; returns nsteps x len(DIAG_COLUMNS) timeseries rows."""
         rows = np.zeros((nsteps, len(DIAG_COLUMNS))) if diagnostics else None
         _check(library().vpd_step(self._h, nsteps, _dp(rows) if diagnostics else None))
         return rows
+
+    def set_surrogate(self, weights=None, biases=None, guess: str = "network",
+                      newton_steps: int = 2):
+        """Attaches the learned return map (material_mode MATERIAL_SURROGATE cases)."""
+        w = None if weights is None else np.ascontiguousarray(weights, dtype=np.uint16)
+        b = None if biases is None else np.ascontiguousarray(biases, dtype=np.float32)
+        _check(library().vpd_set_surrogate(self._h, None if w is None else w.ctypes.data_as(_VP),
+                                           None if b is None else b.ctypes.data_as(_VP),
+                                           GUESS[guess], newton_steps))
 
     def last_step_ms(self) -> float:
         out = ctypes.c_double()

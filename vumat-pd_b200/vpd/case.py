@@ -31,7 +31,7 @@ DIAG_COLUMNS = (
     "engineering_strain", "lateral_strain", "nominal_stress_MPa", "average_axial_strain",
     "average_axial_stress_MPa", "max_eqps", "max_internal_indicator", "kinetic_energy_Nmm",
     "internal_energy_Nmm", "external_work_Nmm", "relative_energy_error",
-    "net_internal_force_N", "finite")
+    "net_internal_force_N", "finite", "plastic_points", "fallback_points")
 DIAG = {name: i for i, name in enumerate(DIAG_COLUMNS)}
 
 FIELDS = ("position", "volume", "displacement", "velocity", "acceleration", "defgrad",

@@ -30,12 +30,27 @@ def main(argv=None):
     ap.add_argument("--warm", type=int, default=2, help="untimed increments first")
     ap.add_argument("--steps", type=int, default=4)
     ap.add_argument("--stage-steps", type=int, default=3)
+    ap.add_argument("--surrogate", choices=("network", "hybrid", "warm_start"),
+                    help="material_mode surrogate with this guess (default: the VUMAT)")
+    ap.add_argument("--newton-steps", type=int, default=2)
+    ap.add_argument("--train-samples", type=int, default=400_000,
+                    help="increments for the network trained before the run")
+    ap.add_argument("--train-epochs", type=int, default=4)
     a = ap.parse_args(argv)
     over = {"nx": a.nx, "precision": 1 if a.precision == "mixed" else 0}
     if a.no_damage:
         over["damage_mode"] = 0
+    weights = (None, None)
+    if a.surrogate:
+        over["material_mode"] = 1
+        if a.surrogate != "warm_start":
+            w, b, _ = vpd.train_surrogate(tensile_bar(a.config).props, samples=a.train_samples,
+                                          epochs=a.train_epochs)
+            weights = (w, b)
     case = tensile_bar(a.config, **over)
     with vpd.Simulation(case) as sim:
+        if a.surrogate:
+            sim.set_surrogate(*weights, guess=a.surrogate, newton_steps=a.newton_steps)
         if a.warm:
             sim.step(a.warm, diagnostics=False)
         ms = None
@@ -44,7 +59,8 @@ def main(argv=None):
             ms = sim.last_step_ms() / a.steps
         stages = sim.profile_stages(a.stage_steps) if a.stage_steps else {}
         print(json.dumps({"config": a.config, "nx": a.nx, "precision": a.precision,
-                          "damage": not a.no_damage, "points": sim.n_points, "bonds": sim.n_bonds,
+                          "damage": not a.no_damage, "surrogate": a.surrogate,
+                          "points": sim.n_points, "bonds": sim.n_bonds,
                           "layout_words": sim.layout_words, "ms_per_increment": ms,
                           "stage_ms": stages}))
 
