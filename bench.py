@@ -1,23 +1,32 @@
 #!/usr/bin/env python
-"""Throughput of the correspondence-PD explicit increment on the 1M-point steel bar.
+"""Throughput of the correspondence-PD explicit increment on the 1M-point steel bar:
+surrogate + mixed-precision PD against plain FP64 PD.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl vpd|reference]
 
-Workload: the 400x50x50 jittered Johnson-Cook tensile bar (1,000,000 points, horizon
-4.015 h, about 238 bonds per point, critical-stretch damage, grips pulled at 5 m/s). A step
-is one explicit increment of the whole bar. One process per GPU (torchrun); the path does not
-shard across GPUs, so N GPUs run N independent replicas ("replicas only") and the value is
-the sum of their particle-steps/s, timed as the max over ranks.
+Workload: the 400x50x50 jittered Johnson-Cook tensile bar (1,000,000 points, horizon 4.015 h,
+about 238 bonds per point, grips pulled at 5 m/s) in plastic flow: each mode runs the bar from
+rest for --preload increments (untimed), W warm-up increments, then K timed increments. The
+bar runs without bond damage: with critical-stretch damage the bar fails near increment 450,
+before it yields, so the damaged bar is timed separately from rest (from_rest_with_damage). A
+step is one explicit increment of the whole bar. One process per GPU (torchrun); the path
+does not shard across GPUs, so N GPUs run N independent replicas ("replicas only") and the
+value is the sum of their particle-steps/s, timed as the max over ranks.
+
+Modes: plain_fp64 (FP64 bonds, the VUMAT's bisection), mixed (FP32 bond sums, the VUMAT),
+surrogate_mixed (the headline: FP32 bond sums, learned return map with the hybrid guess --
+previous plastic increment, else the network trained here by vpd_train_surrogate -- two Newton
+steps, bisection fallback), and two ablations of the guess (network only, warm start only).
 
 Printed JSON line (rank 0):
-  value        particle-steps/s, device time (CUDA events on the library's stream) of K
-               increments after W warm-up increments, inputs resident in HBM
-  e2e          the same K increments through the C ABI as a host driver runs them: the case
-               created from host position/volume arrays, one vpd_step call per increment
-               returning its timeseries row to host memory, and the final snapshot fields
-               copied back; host wall clock
-  roofline     the dominant kernel's algorithmic bytes / its CUDA-event time vs the measured
-               HBM copy bandwidth; traffic from the ncu capture summarised in profiles/
+  value        particle-steps/s of surrogate_mixed, device time (CUDA events on the library's
+               stream) of the K increments, inputs resident in HBM
+  e2e          the whole job of the headline mode through the C ABI with host buffers: case
+               created from host position/volume arrays, network attached from host arrays,
+               all preload+W+K increments in vpd_step calls returning their timeseries rows,
+               final snapshot fields copied back; host wall clock over all increments
+  roofline     the headline mode's dominant kernel: algorithmic bytes / its CUDA-event time
+               vs the measured HBM copy bandwidth; traffic from the ncu summary in profiles/
   cpu_baseline the reference library (compiled from its sources into oracle/_ref) on a
                100k-point slab of the same bar, all host threads
 --impl reference prints the reference library's own line for the same metric.
@@ -48,9 +57,12 @@ def parse_args():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="vpd", choices=("vpd", "reference"))
     p.add_argument("--nx", type=int, default=400, help="bar length in lattice planes")
-    p.add_argument("--plastic-preload", type=int, default=2000,
-                   help="extra measurement after this many increments (0 disables)")
+    p.add_argument("--preload", type=int, default=2000,
+                   help="untimed increments from rest before the timed window (plastic flow)")
     p.add_argument("--cpu-steps", type=int, default=12)
+    p.add_argument("--train-samples", type=int, default=2_000_000)
+    p.add_argument("--train-epochs", type=int, default=20)
+    p.add_argument("--no-ablations", action="store_true", help="skip the guess ablations")
     return p.parse_args()
 
 
@@ -122,26 +134,27 @@ def algorithmic_bytes(nw, damage, mixed):
     through the caches is counted once, with the point that owns it."""
     masks = 4 * nw + (8 * nw if damage else 0)
     force_masks = 4 * nw + (4 * nw if damage else 0)
+    # F_n, V_n, R_n read and written; E, sigma, state read and written; two energies; the
+    # point's x,y,z,V; the observation weight
+    history = 72 * 3 * 2 + 48 * 3 * 2 + 16 * 2 + 32 + 8
     if mixed:
         return {
             # jit, u (float4) of the point; G written (9 floats)
             "deformation": 16 + 16 + 36 + masks,
-            # G (9 floats), K^-1, F_n, V_n, R_n read and written, E, sigma, state, energies,
-            # volume, window weight; V M written as 12 floats
-            "material": 36 + 72 + 72 * 3 * 2 + 48 * 3 * 2 + 16 * 2 + 16 + 48,
-            # jit, V M (12 floats) of the point; f written
-            "force": 16 + 48 + 32 + force_masks,
+            # G (9 floats), K^-1, the history, jit; the force map written (3 float4)
+            "material": 36 + 72 + history + 16 + 48,
+            # jit, force map (3 float4), sum V xi of the point; f written
+            "force": 16 + 48 + 32 + 32 + force_masks,
             # f, u, v, a read; u (FP64 and FP32), v, a written; flags, volume
-            "integrate": 32 + 96 + 96 + 16 + 1 + 8,
+            "integrate": 32 + 96 + 112 + 1 + 8,
         }
     return {
         # x,y,z,V and u of the point, K^-1, F written
         "deformation": 32 + 32 + 72 + 72 + masks,
-        # F, K^-1, F_n, V_n, R_n read and written, E, sigma, state, energies, volume, window
-        # weight; V M written (10 doubles)
-        "material": 72 * 2 + 72 * 3 * 2 + 48 * 3 * 2 + 16 * 2 + 16 + 80,
-        # x,y,z,V and V M of the point; f written
-        "force": 32 + 80 + 32 + force_masks,
+        # F, K^-1, the history; the force map written (3 double4)
+        "material": 72 + 72 + history + 96,
+        # x,y,z,V, force map (3 double4), sum V xi of the point; f written
+        "force": 32 + 96 + 32 + 32 + force_masks,
         "integrate": 32 + 96 + 96 + 1 + 8,
     }
 
@@ -203,7 +216,7 @@ def run_gpu(args, world, rank, local):
     import numpy as np
     import torch
     import vpd
-    from vpd.case import PRECISION_FP64, PRECISION_MIXED, tensile_bar
+    from vpd.case import MATERIAL_SURROGATE, PRECISION_FP64, PRECISION_MIXED, tensile_bar
 
     torch.cuda.set_device(local)
     dist = None
@@ -228,99 +241,118 @@ def run_gpu(args, world, rank, local):
         peak = float(np.max(np.abs(ref)))
         return float(np.sqrt(np.mean((a - ref) ** 2)) / (peak if peak > 0 else 1.0))
 
-    base = tensile_bar(3, nx=args.nx)
-    K, W = args.steps, args.warmup
+    K, W, P = args.steps, args.warmup, args.preload
     stress_col = vpd.DIAG["average_axial_stress_MPa"]
-    modes, clocks = {}, ClockSampler(local)
-    for name, precision in (("plain_fp64", PRECISION_FP64), ("mixed", PRECISION_MIXED)):
-        sim = vpd.Simulation(base.replace(precision=precision))
+    bar = tensile_bar(3, nx=args.nx)
+    flow = bar.replace(damage_mode=0)
+
+    # the network (its training set: increments solved by the device VUMAT)
+    w, b, report = vpd.train_surrogate(bar.props, samples=args.train_samples, epochs=args.train_epochs)
+
+    def run(case, guess=None, preload=P):
+        sim = vpd.Simulation(case)
+        if guess:
+            sim.set_surrogate(*((w, b) if guess != "warm_start" else (None, None)), guess=guess,
+                              newton_steps=2)
         n, nb, nw = sim.n_points, sim.n_bonds / sim.n_points, sim.layout_words
+        if preload:
+            sim.step(preload, diagnostics=False)
         sim.step(W, diagnostics=False)
         barrier()
         rows = sim.step(K, diagnostics=True)
         barrier()
         ms = max_over_ranks(sim.last_step_ms())
-        stages = sim.profile_stages(5)
+        stages = sim.profile_stages(3)
+        fields = {"displacement": sim.field("displacement"), "eqps": sim.field("state")[:, 1].copy()}
         sim.close()
-        modes[name] = {"value": world * n * K / (ms * 1e-3), "ms_per_step": ms / K,
-                       "stage_ms": {k: round(v, 4) for k, v in stages.items()},
-                       "finite": bool(rows[-1, vpd.DIAG["finite"]] == 1.0), "rows": rows}
-    clock = clocks.stop()
-    ref_stress = modes["plain_fp64"]["rows"][:, stress_col]
-    for name, m in modes.items():
-        m["stress_nrmse_vs_fp64"] = nrmse(m.pop("rows")[:, stress_col], ref_stress)
-    eligible = [k for k, m in modes.items() if m["stress_nrmse_vs_fp64"] <= 5e-3 and m["finite"]]
-    best = max(eligible, key=lambda k: modes[k]["value"])
-    precision = PRECISION_MIXED if best == "mixed" else PRECISION_FP64
-    case = base.replace(precision=precision)
+        plastic = rows[:, vpd.DIAG["plastic_points"]].sum()
+        fallback = rows[:, vpd.DIAG["fallback_points"]].sum()
+        return {"value": world * n * K / (ms * 1e-3), "ms_per_step": ms / K,
+                "stage_ms": {k: round(v, 4) for k, v in stages.items()},
+                "finite": bool(rows[-1, vpd.DIAG["finite"]] == 1.0),
+                "plastic_points_per_step": float(plastic / K),
+                "fallback_fraction": float(fallback / plastic) if plastic else 0.0,
+                "max_eqps": float(rows[-1, vpd.DIAG["max_eqps"]]),
+                "rows": rows, "fields": fields, "n": n, "nb": nb, "nw": nw}
 
-    # end to end through the C ABI with host buffers, in the headline mode
-    positions = vpd.Simulation(base.replace(precision=PRECISION_FP64))
+    surrogate = flow.replace(precision=PRECISION_MIXED, material_mode=MATERIAL_SURROGATE)
+    clocks = ClockSampler(local)
+    modes = {"plain_fp64": run(flow.replace(precision=PRECISION_FP64)),
+             "mixed": run(flow.replace(precision=PRECISION_MIXED)),
+             "surrogate_mixed": run(surrogate, "hybrid")}
+    if not args.no_ablations:
+        modes["surrogate_network_only_mixed"] = run(surrogate, "network")
+        modes["surrogate_warm_start_only_mixed"] = run(surrogate, "warm_start")
+    damaged = {"plain_fp64": run(bar.replace(precision=PRECISION_FP64), preload=0),
+               "surrogate_mixed": run(bar.replace(precision=PRECISION_MIXED,
+                                                  material_mode=MATERIAL_SURROGATE), "hybrid", preload=0)}
+    clock = clocks.stop()
+    for group in (modes, damaged):
+        base = group["plain_fp64"]
+        for m in group.values():
+            m["stress_nrmse_vs_fp64"] = nrmse(m["rows"][:, stress_col], base["rows"][:, stress_col])
+            du = m["fields"]["displacement"] - base["fields"]["displacement"]
+            m["displacement_nrmse_vs_fp64"] = float(
+                np.sqrt(np.mean(du ** 2)) / max(np.abs(base["fields"]["displacement"]).max(), 1e-300))
+            m["eqps_max_abs_error_vs_fp64"] = float(np.abs(m["fields"]["eqps"] - base["fields"]["eqps"]).max())
+    ref, head = modes["plain_fp64"], modes["surrogate_mixed"]
+    n, nb, nw = head["n"], head["nb"], head["nw"]
+
+    # end to end through the C ABI with host buffers: the headline mode's whole job
+    positions = vpd.Simulation(flow.replace(precision=PRECISION_FP64))
     host_pos, host_vol = positions.field("position"), positions.field("volume")[:, 0].copy()
     positions.close()
+    total = P + W + K
     barrier()
     t0 = time.perf_counter()
-    e2e_sim = vpd.Simulation(case, positions=host_pos, volumes=host_vol)
-    for _ in range(K):
-        e2e_sim.step(1, diagnostics=True)
+    e2e_sim = vpd.Simulation(surrogate, positions=host_pos, volumes=host_vol)
+    e2e_sim.set_surrogate(w, b, guess="hybrid", newton_steps=2)
+    e2e_rows = 0
+    for done in range(0, total, 256):
+        e2e_rows += e2e_sim.step(min(256, total - done), diagnostics=True).nbytes
     snap = [e2e_sim.field(f) for f in ("displacement", "velocity", "stress_spatial", "state")]
     e2e_s = max_over_ranks(time.perf_counter() - t0)
     e2e_sim.close()
-    h2d = host_pos.nbytes + host_vol.nbytes
-    d2h = sum(a.nbytes for a in snap) + K * len(vpd.DIAG_COLUMNS) * 8
-
-    # the plastic regime: the same bar without damage (with damage the bar fails at ~450
-    # increments), after a preload, in both modes
-    plastic = None
-    if args.plastic_preload > 0:
-        plastic = {"workload": "tensile_bar_3 without damage", "start_increment": args.plastic_preload + 1}
-        prow = {}
-        for name, prec in (("plain_fp64", PRECISION_FP64), ("mixed", PRECISION_MIXED)):
-            ps = vpd.Simulation(base.replace(precision=prec, damage_mode=0))
-            ps.step(args.plastic_preload, diagnostics=False)
-            r = ps.step(K, diagnostics=True)
-            pms = max_over_ranks(ps.last_step_ms())
-            prow[name] = r
-            plastic[name] = {"value": world * n * K / (pms * 1e-3), "ms_per_step": pms / K,
-                             "max_eqps": float(r[-1, vpd.DIAG["max_eqps"]]),
-                             "stage_ms": {k: round(v, 4) for k, v in ps.profile_stages(3).items()}}
-            ps.close()
-        plastic["mixed"]["stress_nrmse_vs_fp64"] = nrmse(prow["mixed"][:, stress_col],
-                                                         prow["plain_fp64"][:, stress_col])
+    h2d = host_pos.nbytes + host_vol.nbytes + w.nbytes + b.nbytes
+    d2h = sum(a.nbytes for a in snap) + e2e_rows
 
     if rank != 0:
         if dist:
             dist.destroy_process_group()
         return
     peak, peak_kind = measured_peaks()
-    damage = case.damage_mode == 1
-    alg = algorithmic_bytes(nw, damage, best == "mixed")
-    stages = modes[best]["stage_ms"]
+    alg = algorithmic_bytes(nw, False, True)
+    stages = head["stage_ms"]
     dominant = max(stages, key=stages.get)
     achieved = alg[dominant] * n / (stages[dominant] * 1e-3) / 1e9
     traffic = ncu_traffic()
-    tr = None
-    key = f"{best}:{dominant}"
-    if traffic and key in traffic.get("bytes_per_point", {}):
-        tr = traffic["bytes_per_point"][key] * n
-    ms_step = modes[best]["ms_per_step"]
-    value = modes[best]["value"]
+    key = f"mixed:{dominant}"
+    tr = traffic["bytes_per_point"][key] * n if traffic and key in traffic.get("bytes_per_point", {}) else None
+    ms_step = head["ms_per_step"]
     step_alg = sum(alg.values()) * n
-    survey = survey_bytes(nb, damage) * n
+    survey = survey_bytes(nb, False) * n
     cpu = cpu_reference(args.cpu_steps, 2)
+    for group in (modes, damaged):
+        for m in group.values():
+            for k in ("rows", "fields", "n", "nb", "nw"):
+                m.pop(k)
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+        "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32 bonds / f64 state" if best == "mixed" else "f64", "data": "synthetic",
-        "config": {"workload": "tensile_bar_3: 400x50x50 jittered (+-0.05 h) steel Johnson-Cook "
-                               "bar, horizon 4.015 h, critical stretch 0.02, grips 5 m/s",
-                   "points": n, "bonds_per_point": round(nb, 2), "mode": best,
-                   "material": "device Johnson-Cook VUMAT", "bond_layout_words": nw,
-                   "increments": f"{W + 1}-{W + K} from rest",
+        "dtype": "f32 bonds / f64 state, bf16 network", "data": "synthetic",
+        "config": {"workload": "tensile_bar_3 in plastic flow: 400x50x50 jittered (+-0.05 h) steel "
+                               "Johnson-Cook bar, horizon 4.015 h, grips 5 m/s, no bond damage",
+                   "points": n, "bonds_per_point": round(nb, 2), "mode": "surrogate_mixed",
+                   "material": "learned return map (hybrid guess, 2 Newton steps, VUMAT fallback)",
+                   "bond_layout_words": nw, "increments": f"{P + W + 1}-{P + W + K} from rest",
                    "l2": "working set ~3 GB > 126 MB L2, no flush needed",
                    "parallelism": f"replicas x{world}"},
+        "plain_fp64_value": ref["value"],
+        "speedup_vs_plain_fp64": head["value"] / ref["value"],
         "modes": modes,
-        "plastic_regime": plastic,
+        "from_rest_with_damage": damaged,
+        "surrogate_training": {"final_epoch_loss": report["epoch_loss"][-1],
+                               **{k: v for k, v in report.items() if k != "epoch_loss"}},
         "roofline": {"kernel": dominant, "bound": "hbm", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
                      "traffic": tr, "algorithmic_bytes": alg[dominant] * n},
@@ -330,11 +362,12 @@ def run_gpu(args, world, rank, local):
                           "index_formulation_bytes": survey,
                           "index_formulation_frac": survey / (ms_step * 1e-3) / 1e9 / peak},
         "cpu_baseline": {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")},
-        "e2e": {"value": world * n * K / e2e_s, "unit": UNIT,
-                "h2d_bytes_per_step": h2d / K, "d2h_bytes_per_step": d2h / K,
-                "includes": "vpd_create from host arrays (neighbour search, K^-1), K increments "
-                            "from rest one call each with their rows read back, final snapshot "
-                            "download"},
+        "e2e": {"value": world * n * total / e2e_s, "unit": UNIT,
+                "h2d_bytes_per_step": h2d / total, "d2h_bytes_per_step": d2h / total,
+                "includes": f"vpd_create from host arrays (neighbour search, K^-1), network "
+                            f"attached from host arrays, {total} increments from rest in "
+                            f"vpd_step calls of 256 with their rows read back, final snapshot "
+                            f"download"},
         "gpu_launches": 4 * K,
         "clocks": clock,
     }

@@ -10,7 +10,11 @@
 // A point without a bond in a slot still reads i + delta (clamped to the array) so the warp's
 // loads stay one contiguous range, and its contribution is masked to zero.
 //
-// Stencil slots are ordered by offset (ascending delta for the patches the reference builds).
+// Stencil slots are grouped by the (x, z) components of the offset: the offsets of one group
+// differ only in y, take consecutive slots in ascending y (gaps in y become padding slots whose
+// bits are never set), and a group never straddles a 32-bit word, so one word load and a
+// shift give a point's bits of one group. The tiled bond kernels (vpd_tiled.cu) walk the
+// groups; the slot kernels below walk the slots.
 // Bond stretch is symmetric bit for bit ((i,j) and (j,i) see y and -y, xi and -xi), so the
 // critical-stretch test runs once per pair, by the point with the lower index ("forward"
 // slots, delta > 0), which sets the broken bit of both directed bonds.
@@ -133,38 +137,48 @@ int build_stencil(const int64_t *row_ptr, const int32_t *col, int64_t n, int ny,
   VPD_CUDA(cudaMemcpyAsync(used.data(), table, sizeof(int) * ex.size(), cudaMemcpyDeviceToHost, s));
   VPD_CUDA(cudaStreamSynchronize(s));
   std::vector<int> slot(ex.size(), -1);
-  std::vector<int32_t> delta;
-  std::vector<int> codes;
+  std::vector<int4> groups;  // (dx, dz, lowest dy, (slots << 16) | first slot)
+  int S = 0;                 // slots including padding
   for (int dx = -ex.rx; dx <= ex.rx; ++dx)
-    for (int dy = -ex.ry; dy <= ex.ry; ++dy)
-      for (int dz = -ex.rz; dz <= ex.rz; ++dz) {
-        const int c = ex.code(dx, dy, dz);
-        if (!used[c])
-          continue;
-        slot[c] = (int)delta.size();
-        delta.push_back((dx * ny + dy) * nz + dz);
-        codes.push_back(c);
-      }
-  const int S = (int)delta.size();
+    for (int dz = -ex.rz; dz <= ex.rz; ++dz) {
+      int lo = ex.ry + 1, hi = -ex.ry - 1;
+      for (int dy = -ex.ry; dy <= ex.ry; ++dy)
+        if (used[ex.code(dx, dy, dz)])
+          lo = std::min(lo, dy), hi = std::max(hi, dy);
+      if (lo > hi)
+        continue;
+      const int count = hi - lo + 1;
+      if ((S & 31) + count > 32)
+        S = (S + 31) & ~31;  // start the group in the next word
+      for (int dy = lo; dy <= hi; ++dy)
+        if (used[ex.code(dx, dy, dz)])
+          slot[ex.code(dx, dy, dz)] = S + (dy - lo);
+      groups.push_back(make_int4(dx, dz, lo, (count << 16) | S));
+      S += count;
+    }
   if (S == 0 || S > 32 * kMaxStencilWords) {
     cudaFree(dext), cudaFree(table);
     return VPD_OK;
   }
   const int nw = (S + 31) / 32;
-  std::vector<int32_t> reverse(32 * nw, -1);
+  std::vector<int32_t> delta(32 * nw, 0), reverse(32 * nw, -1);
   std::vector<uint32_t> forward(nw, 0u);
   std::vector<float4> e0(32 * nw, make_float4(0.f, 0.f, 0.f, 0.f));
-  for (int sl = 0; sl < S; ++sl) {
-    const int c = codes[sl];
-    const int dz = c % (2 * ex.rz + 1) - ex.rz;
-    const int dy = (c / (2 * ex.rz + 1)) % (2 * ex.ry + 1) - ex.ry;
-    const int dx = c / ((2 * ex.rz + 1) * (2 * ex.ry + 1)) - ex.rx;
-    reverse[sl] = slot[ex.code(-dx, -dy, -dz)];  // bonds come in pairs, so it exists
-    if (delta[sl] > 0)
-      forward[sl >> 5] |= 1u << (sl & 31);
-    e0[sl] = make_float4((float)(dx * spacing), (float)(dy * spacing), (float)(dz * spacing), 0.f);
-  }
-  delta.resize(32 * nw, 0);
+  for (int dx = -ex.rx; dx <= ex.rx; ++dx)
+    for (int dy = -ex.ry; dy <= ex.ry; ++dy)
+      for (int dz = -ex.rz; dz <= ex.rz; ++dz) {
+        const int sl = slot[ex.code(dx, dy, dz)];
+        if (sl < 0)
+          continue;
+        delta[sl] = (dx * ny + dy) * nz + dz;
+        reverse[sl] = slot[ex.code(-dx, -dy, -dz)];  // bonds come in pairs, so it exists
+        if (delta[sl] > 0)
+          forward[sl >> 5] |= 1u << (sl & 31);
+        e0[sl] = make_float4((float)(dx * spacing), (float)(dy * spacing), (float)(dz * spacing), 0.f);
+      }
+  for (int sl = 0; sl < 32 * nw; ++sl)
+    if (reverse[sl] < 0)
+      reverse[sl] = sl;  // padding slots
   VPD_CUDA(cudaMalloc(&slot_of, sizeof(int) * ex.size()));
   VPD_CUDA(cudaMemcpyAsync(slot_of, slot.data(), sizeof(int) * ex.size(), cudaMemcpyHostToDevice, s));
   VPD_CUDA(cudaMalloc(&st.delta, sizeof(int32_t) * 32 * nw));
@@ -178,6 +192,8 @@ int build_stencil(const int64_t *row_ptr, const int32_t *col, int64_t n, int ny,
   VPD_CUDA(cudaMemsetAsync(st.broken, 0, sizeof(uint32_t) * nw * n, s));
   VPD_CUDA(cudaMalloc(&st.e0, sizeof(float4) * 32 * nw));
   VPD_CUDA(cudaMemcpyAsync(st.e0, e0.data(), sizeof(float4) * 32 * nw, cudaMemcpyHostToDevice, s));
+  VPD_CUDA(cudaMalloc(&st.groups, sizeof(int4) * groups.size()));
+  VPD_CUDA(cudaMemcpyAsync(st.groups, groups.data(), sizeof(int4) * groups.size(), cudaMemcpyHostToDevice, s));
   VPD_CUDA(cudaMemsetAsync(dext, 0, sizeof(int), s));
   k_mask_build<<<blocks, 256, 0, s>>>(row_ptr, col, n, ny, nz, ex, slot_of, st.delta, nw, st.mask, dext);
   int bad = 0;
@@ -190,12 +206,13 @@ int build_stencil(const int64_t *row_ptr, const int32_t *col, int64_t n, int ny,
   }
   st.slots = S;
   st.nw = nw;
+  st.ngroups = (int)groups.size();
   return VPD_OK;
 }
 
 void free_stencil(StencilLayout &st) {
   cudaFree(st.delta), cudaFree(st.reverse), cudaFree(st.forward), cudaFree(st.mask), cudaFree(st.broken);
-  cudaFree(st.e0);
+  cudaFree(st.e0), cudaFree(st.groups);
   st = StencilLayout{};
 }
 

@@ -489,7 +489,7 @@ int integrate_grid(int64_t n) { return (int)((n + kBondThreads - 1) / kBondThrea
 int launch_stage(int stage, const StepParams &p, cudaStream_t s) {
   if (stage == 0) {
     if (p.mixed)
-      return launch_deformation_mixed(p, s);
+      return p.tiled ? launch_deformation_tiled(p, s) : launch_deformation_mixed(p, s);
     if (p.st.nw)
       return launch_deformation_stencil(p, s);
     k_deformation<<<bond_grid(p.n), kBondThreads, 0, s>>>(p);
@@ -499,7 +499,7 @@ int launch_stage(int stage, const StepParams &p, cudaStream_t s) {
     k_material<<<(unsigned)material_grid(p.n), kMaterialThreads, 0, s>>>(p);
   } else if (stage == 2) {
     if (p.mixed)
-      return launch_force_mixed(p, s);
+      return p.tiled ? launch_force_tiled(p, s) : launch_force_mixed(p, s);
     if (p.st.nw)
       return launch_force_stencil(p, s);
     k_force<<<bond_grid(p.n), kBondThreads, 0, s>>>(p);

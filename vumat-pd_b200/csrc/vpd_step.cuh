@@ -28,7 +28,8 @@ constexpr int kMaxStencilWords = 32; // at most 1024 lattice offsets per stencil
 
 // Lattice-stencil bond layout (vpd_stencil.cu). nw == 0: not in use.
 struct StencilLayout {
-  int slots = 0, nw = 0;
+  int slots = 0, nw = 0, ngroups = 0;
+  int4 *groups = nullptr;      // [ngroups] (dx, dz, lowest dy, (slots << 16) | first slot)
   int32_t *delta = nullptr;    // [32 nw] index difference j - i of each slot (0: padding)
   int32_t *reverse = nullptr;  // [32 nw] slot of the opposite offset
   uint32_t *forward = nullptr; // [nw] bits of the slots with delta > 0
@@ -47,6 +48,10 @@ struct StepParams {
   const int32_t *sell;        // sliced-ELL neighbour indices
   uint32_t *words;            // broken-bond bits, one word per (slice, column)
   StencilLayout st;           // lattice-stencil layout; used instead of the ELL when st.nw > 0
+  int lat_nx, lat_ny, lat_nz; // the lattice (points in index order (x ny + y) nz + z)
+  double lat_h;               // lattice spacing
+  int tiled;                  // mixed precision: points per thread of the tiled bond kernels
+                              // (2 or 3), 0 for the per-slot kernels
   // kinematic state
   double4 *u0, *u1;           // displacement ping-pong: increment s reads u[s & 1]
   double4 *vel, *acc, *force;
@@ -117,5 +122,8 @@ int launch_deformation_mixed(const StepParams &p, cudaStream_t s);
 int launch_force_mixed(const StepParams &p, cudaStream_t s);
 int launch_mixed_setup(const StepParams &p, int ny, int nz, double h, double yoff, double zoff,
                        cudaStream_t s);
+// tiled mixed-precision bond kernels (vpd_tiled.cu)
+int launch_deformation_tiled(const StepParams &p, cudaStream_t s);
+int launch_force_tiled(const StepParams &p, cudaStream_t s);
 
 }  // namespace vpd
