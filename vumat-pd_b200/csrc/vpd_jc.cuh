@@ -31,15 +31,27 @@ inline JcParams make_jc_params(const double *props) {
   return p;
 }
 
-// Flow stress (JohnsonCook.f90:160-170).
-__device__ __forceinline__ double jc_yield(const JcParams &p, double ep, double rate,
-                                           double temp) {
+// Flow stress (JohnsonCook.f90:160-170), split so that a return map evaluates the thermal
+// factor once (the temperature stays the old one during a return) and pays one pow and one log
+// per iteration. The values are bit for bit those of the one-line formula: pow(x, 1) is x and
+// log(rate0 / rate0) is 0 exactly, so the m = 1 and zero-rate shortcuts change nothing.
+__device__ __forceinline__ double jc_thermal(const JcParams &p, double temp) {
   double theta = (temp - p.tref) / (p.tmelt - p.tref);
   theta = theta > 0.0 ? theta : 0.0;
   theta = theta < 1.0 ? theta : 1.0;
-  const double effectiveRate = rate == 0.0 ? p.rate0 : rate;
-  return (p.a0 + p.b0 * pow(ep, p.hardN)) * (1.0 - pow(theta, p.thermalM)) *
-         (1.0 + p.rateC * log(effectiveRate / p.rate0));
+  return 1.0 - (p.thermalM == 1.0 ? theta : pow(theta, p.thermalM));
+}
+__device__ __forceinline__ double jc_rate_term(const JcParams &p, double rate) {
+  return rate == 0.0 ? 1.0 : 1.0 + p.rateC * log(rate / p.rate0);
+}
+__device__ __forceinline__ double jc_flow(const JcParams &p, double hardPow, double thermal, double rterm) {
+  return (p.a0 + p.b0 * hardPow) * thermal * rterm;
+}
+__device__ __forceinline__ double jc_yield_t(const JcParams &p, double ep, double rate, double thermal) {
+  return jc_flow(p, pow(ep, p.hardN), thermal, jc_rate_term(p, rate));
+}
+__device__ __forceinline__ double jc_yield(const JcParams &p, double ep, double rate, double temp) {
+  return jc_yield_t(p, ep, rate, jc_thermal(p, temp));
 }
 
 struct JcPoint {
@@ -53,6 +65,7 @@ struct JcPoint {
 struct JcTrial {
   double trial[6], dev[6];
   double pressure, qTrial, epOld, temperature, oldYield;
+  double thermal;  // 1 - theta^m at the old temperature
 };
 
 // Forms the trial state. On the first (initialising) call it completes the update of pt
@@ -75,6 +88,7 @@ __device__ __forceinline__ bool jc_trial(const JcParams &p, const double *inc, J
     return false;
   }
   t.epOld = pt.state[1], t.temperature = pt.state[2], t.oldYield = pt.state[3];
+  t.thermal = jc_thermal(p, t.temperature);
   t.pressure = (t.trial[0] + t.trial[1] + t.trial[2]) / 3.0;
 #pragma unroll
   for (int i = 0; i < 3; ++i)
@@ -96,7 +110,7 @@ __device__ __forceinline__ int jc_bisection(const JcParams &p, double dt, const 
   while (iteration < 50) {
     ++iteration;
     const double epRate = epInc / dt;
-    yield = jc_yield(p, t.epOld + epInc, epRate, t.temperature);
+    yield = jc_yield_t(p, t.epOld + epInc, epRate, t.thermal);
     yield = yield > t.oldYield ? yield : t.oldYield;
     double qNew = t.qTrial - 3.0 * p.mu * epInc;
     qNew = qNew > 0.0 ? qNew : 0.0;

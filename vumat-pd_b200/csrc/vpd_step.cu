@@ -175,7 +175,10 @@ __global__ void __launch_bounds__(kBondThreads) k_deformation(StepParams p) {
 }
 
 // ------------------------------------------------------------------ k_material
-__global__ void __launch_bounds__(kMaterialThreads) k_material(const __grid_constant__ StepParams p) {
+// Four blocks per SM (128 registers, a few hundred bytes of spills to L1): the FP64 kinematics
+// and return map are latency-bound, and the extra warps outweigh the spills (26 % faster on
+// the 250k-point bar in plastic flow than at the unconstrained 196 registers).
+__global__ void __launch_bounds__(kMaterialThreads, 4) k_material(const __grid_constant__ StepParams p) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   double part[PM_COUNT] = {};
   double maxEqps = 0.0;

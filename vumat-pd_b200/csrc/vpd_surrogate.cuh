@@ -63,33 +63,29 @@ __device__ __forceinline__ void surrogate_features(const JcParams &p, double dt,
 
 // Yield stress of the trial state at epInc = 0, as the bisection's first iteration takes it.
 __device__ __forceinline__ double jc_yield0(const JcParams &p, const JcTrial &t) {
-  const double y = jc_yield(p, t.epOld, 0.0, t.temperature);
+  const double y = jc_yield_t(p, t.epOld, 0.0, t.thermal);
   return y > t.oldYield ? y : t.oldYield;
 }
 
-// r(x) with its slope. The residual is formed exactly as in the bisection (jc_yield, floor at
-// oldYield, qNew clipped at 0); the slope differentiates the hardening term B n ep^(n-1) and
-// the rate term C / x (zero at x = 0, where the VUMAT uses the reference rate).
+// r(x) with its slope. The residual is formed exactly as in the bisection (the same flow
+// stress arithmetic, floor at oldYield, qNew clipped at 0) with one pow and one log; the slope
+// differentiates the hardening term B n ep^(n-1) = B n ep^n / ep and the rate term C / x (zero
+// at x = 0, where the VUMAT uses the reference rate).
 __device__ __forceinline__ double jc_residual(const JcParams &p, double dt, const JcTrial &t, double x,
                                               double &slope, double &yield) {
   const double ep = t.epOld + x, rate = x / dt;
-  const double y = jc_yield(p, ep, rate, t.temperature);
+  const double hp = pow(ep, p.hardN), rterm = jc_rate_term(p, rate);
+  const double y = jc_flow(p, hp, t.thermal, rterm);
   yield = y > t.oldYield ? y : t.oldYield;
   double qNew = t.qTrial - 3.0 * p.mu * x;
   const bool clipped = qNew <= 0.0;
   qNew = clipped ? 0.0 : qNew;
   double dy = 0.0;
   if (y > t.oldYield) {
-    double theta = (t.temperature - p.tref) / (p.tmelt - p.tref);
-    theta = theta > 0.0 ? theta : 0.0;
-    theta = theta < 1.0 ? theta : 1.0;
-    const double thermal = 1.0 - pow(theta, p.thermalM);
-    const double eff = rate == 0.0 ? p.rate0 : rate;
-    const double hard = p.a0 + p.b0 * pow(ep, p.hardN);
-    const double rterm = 1.0 + p.rateC * log(eff / p.rate0);
-    const double dhard = ep > 0.0 ? p.b0 * p.hardN * pow(ep, p.hardN - 1.0) : 0.0;
+    const double hard = p.a0 + p.b0 * hp;
+    const double dhard = ep > 0.0 ? p.b0 * p.hardN * hp / ep : 0.0;
     const double drate = rate == 0.0 ? 0.0 : p.rateC / x;
-    dy = (dhard * rterm + hard * drate) * thermal;
+    dy = (dhard * rterm + hard * drate) * t.thermal;
   }
   slope = (clipped ? 0.0 : -3.0 * p.mu) - dy;
   return qNew - yield;
