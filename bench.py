@@ -230,12 +230,7 @@ def run_gpu(args, world, rank, local):
         if dist:
             dist.barrier()
 
-    def max_over_ranks(x):
-        if not dist:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    from vpd.replicas import job_throughput, max_over_ranks
 
     def nrmse(a, ref):
         peak = float(np.max(np.abs(ref)))
@@ -267,7 +262,7 @@ def run_gpu(args, world, rank, local):
         sim.close()
         plastic = rows[:, vpd.DIAG["plastic_points"]].sum()
         fallback = rows[:, vpd.DIAG["fallback_points"]].sum()
-        return {"value": world * n * K / (ms * 1e-3), "ms_per_step": ms / K,
+        return {"value": job_throughput(n, K, ms, world), "ms_per_step": ms / K,
                 "stage_ms": {k: round(v, 4) for k, v in stages.items()},
                 "finite": bool(rows[-1, vpd.DIAG["finite"]] == 1.0),
                 "plastic_points_per_step": float(plastic / K),
@@ -362,7 +357,7 @@ def run_gpu(args, world, rank, local):
                           "index_formulation_bytes": survey,
                           "index_formulation_frac": survey / (ms_step * 1e-3) / 1e9 / peak},
         "cpu_baseline": {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")},
-        "e2e": {"value": world * n * total / e2e_s, "unit": UNIT,
+        "e2e": {"value": job_throughput(n, total, e2e_s * 1e3, world), "unit": UNIT,
                 "h2d_bytes_per_step": h2d / total, "d2h_bytes_per_step": d2h / total,
                 "includes": f"vpd_create from host arrays (neighbour search, K^-1), network "
                             f"attached from host arrays, {total} increments from rest in "
