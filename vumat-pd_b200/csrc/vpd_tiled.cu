@@ -4,11 +4,17 @@
 //
 // The stencil's slots are grouped by the offset's (x, z) components (vpd_stencil.cu): the
 // offsets of a group differ only in y, so the neighbours that the kTileP points reach through
-// one group form a single run of cnt + kTileP - 1 consecutive lattice points along y. The
-// thread loads each of those neighbour records once and applies it to every one of its
-// points that has the matching bond, instead of loading it once per bond: the loads fall by
-// about cnt kTileP / (cnt + kTileP - 1). Consecutive threads take consecutive z, so each load
-// of a warp is one contiguous range.
+// one group form a single run of cnt + kTileP - 1 consecutive lattice points along y (the
+// group's window). The thread loads each neighbour record of the window once and applies it
+// to every one of its points that has the matching bond: the loads fall by about
+// cnt kTileP / (cnt + kTileP - 1). Consecutive threads take consecutive z, so each load of a
+// warp is one contiguous range.
+//
+// A group's window is walked fully unrolled for each slot count up to kUnrolledSlots (a switch
+// over the count picks the instance): which (window position, point) pairs hold a slot, the
+// bit each one tests and the lattice offset along y are then compile-time constants, and the
+// neighbour index is 32-bit. Larger groups, and lattices of 2^30 points or more, take the same
+// body in a runtime loop with 64-bit indices.
 //
 // Arithmetic is that of vpd_mixed.cu: FP32 bond terms, per-group partial sums (folded with
 // Kahan compensation into the force), the FP32 stretch test with a 1e-5 margin and the exact
@@ -17,7 +23,10 @@
 
 namespace vpd {
 
-// Lattice coordinates of thread tau's column: z fastest, then the y-block, then x.
+constexpr int kUnrolledSlots = 12;  // the switches below list counts 1 .. 12
+
+// Lattice coordinates of thread tau's column: z fastest, then the y-block, then x. Threads
+// past the lattice get the last column (their points are marked invalid).
 template <int kTileP>
 __device__ __forceinline__ bool tile_coords(const StepParams &p, int64_t tau, int &x, int &yb, int &z) {
   const int nz = p.lat_nz, nyb = (p.lat_ny + kTileP - 1) / kTileP;
@@ -25,14 +34,81 @@ __device__ __forceinline__ bool tile_coords(const StepParams &p, int64_t tau, in
   const int64_t r = tau / nz;
   yb = (int)(r % nyb);
   x = (int)(r / nyb);
-  return x < p.lat_nx;
+  const bool inb = x < p.lat_nx;
+  x = inb ? x : p.lat_nx - 1;
+  return inb;
 }
 
 __device__ __forceinline__ uint32_t group_bits(uint32_t word, int shift, uint32_t cm) {
   return (word >> shift) & cm;
 }
 
-template <bool DAMAGE, int kTileP>
+template <typename I> __device__ __forceinline__ I clamp_to(I j, I n) { return j < 0 ? 0 : (j >= n ? n - 1 : j); }
+
+// ------------------------------------------------------------------ deformation
+template <int P> struct DeformPoints {
+  float jx[P], jy[P], jz[P], ux[P], uy[P], uz[P];  // jy includes q h (y relative to the tile's base row)
+};
+
+// One window position t of a group: the neighbour record and its bonds to the tile's points.
+template <bool DAMAGE, int P, typename I>
+__device__ __forceinline__ void deform_element(const StepParams &p, int t, int cnt, I j, float gx, float gz,
+                                               float by0, float h, const DeformPoints<P> &pt,
+                                               const uint32_t (&bits)[P], const uint32_t (&live)[P],
+                                               float (&part)[P][9], uint32_t (&fresh)[P], uint32_t (&near)[P]) {
+  const float4 a = ldgf4(p.jit + j), b = ldgf4(p.uf + j);
+  const float bx = a.x + gx, by = a.y + fmaf((float)t, h, by0), bz = a.z + gz;
+  const float lo = 1.0f - 1.0e-5f, hi = 1.0f + 1.0e-5f;
+#pragma unroll
+  for (int q = 0; q < P; ++q) {
+    if (t < q || t - q >= cnt)  // window position t holds no slot of point q
+      continue;
+    const float e0 = bx - pt.jx[q], e1 = by - pt.jy[q], e2 = bz - pt.jz[q];
+    const float d0 = b.x - pt.ux[q], d1 = b.y - pt.uy[q], d2 = b.z - pt.uz[q];
+    const float v = (bits[q] & (1u << t)) ? a.w : 0.0f;  // no bond: no contribution
+    const float w0 = v * d0, w1 = v * d1, w2 = v * d2;
+    part[q][0] += w0 * e0, part[q][1] += w0 * e1, part[q][2] += w0 * e2;
+    part[q][3] += w1 * e0, part[q][4] += w1 * e1, part[q][5] += w1 * e2;
+    part[q][6] += w2 * e0, part[q][7] += w2 * e1, part[q][8] += w2 * e2;
+    if (DAMAGE && (live[q] & (1u << t))) {
+      const float y0 = e0 + d0, y1 = e1 + d1, y2 = e2 + d2;
+      const float yy = y0 * y0 + y1 * y1 + y2 * y2;
+      const float xx = e0 * e0 + e1 * e1 + e2 * e2;
+      const float tt = p.tension2f * xx;
+      if (yy > tt * hi)
+        fresh[q] |= 1u << t;
+      else if (yy >= tt * lo)
+        near[q] |= 1u << t;
+      else if (p.use_compression) {
+        const float c = p.compression2f * xx;
+        if (yy < c * lo)
+          fresh[q] |= 1u << t;
+        else if (yy <= c * hi)
+          near[q] |= 1u << t;
+      }
+    }
+  }
+}
+
+// The window of one group: CNT > 0 unrolled with 32-bit indices, CNT == 0 a runtime loop.
+template <int CNT, bool DAMAGE, int P, typename I>
+__device__ __forceinline__ void deform_window(const StepParams &p, int cnt, I jb, I nz, I n, float gx, float gz,
+                                              float by0, float h, const DeformPoints<P> &pt,
+                                              const uint32_t (&bits)[P], const uint32_t (&live)[P],
+                                              float (&part)[P][9], uint32_t (&fresh)[P], uint32_t (&near)[P]) {
+  if constexpr (CNT > 0) {
+#pragma unroll
+    for (int t = 0; t < CNT + P - 1; ++t)
+      deform_element<DAMAGE, P, I>(p, t, CNT, clamp_to<I>(jb + (I)t * nz, n), gx, gz, by0, h, pt, bits, live,
+                                   part, fresh, near);
+  } else {
+    for (int t = 0; t < cnt + P - 1; ++t)
+      deform_element<DAMAGE, P, I>(p, t, cnt, clamp_to<I>(jb + (I)t * nz, n), gx, gz, by0, h, pt, bits, live,
+                                   part, fresh, near);
+  }
+}
+
+template <bool DAMAGE, int kTileP, bool UNROLL>
 __global__ void __launch_bounds__(kBondThreads, 2) k_deformation_tiled(const __grid_constant__ StepParams p) {
   const int64_t n = p.n;
   const int ny = p.lat_ny, nz = p.lat_nz;
@@ -41,15 +117,15 @@ __global__ void __launch_bounds__(kBondThreads, 2) k_deformation_tiled(const __g
   const bool inb = tile_coords<kTileP>(p, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, x, yb, z);
   int64_t ip[kTileP];
   bool vp[kTileP];
-  float jx[kTileP], jy[kTileP], jz[kTileP], ux[kTileP], uy[kTileP], uz[kTileP];
+  DeformPoints<kTileP> pt;
 #pragma unroll
   for (int q = 0; q < kTileP; ++q) {
     const int y = yb * kTileP + q;
     vp[q] = inb && y < ny;
     ip[q] = vp[q] ? ((int64_t)x * ny + y) * nz + z : 0;
     const float4 a = ldgf4(p.jit + ip[q]), b = ldgf4(p.uf + ip[q]);
-    jx[q] = a.x, jy[q] = a.y + (float)q * h, jz[q] = a.z;  // y relative to the tile's base row
-    ux[q] = b.x, uy[q] = b.y, uz[q] = b.z;
+    pt.jx[q] = a.x, pt.jy[q] = a.y + (float)q * h, pt.jz[q] = a.z;
+    pt.ux[q] = b.x, pt.uy[q] = b.y, pt.uz[q] = b.z;
   }
   float G[kTileP][9];
 #pragma unroll
@@ -57,7 +133,6 @@ __global__ void __launch_bounds__(kBondThreads, 2) k_deformation_tiled(const __g
 #pragma unroll
     for (int c = 0; c < 9; ++c)
       G[q][c] = 0.0f;
-  const float lo = 1.0f - 1.0e-5f, hi = 1.0f + 1.0e-5f;
   for (int g = 0; g < p.st.ngroups; ++g) {
     const int4 gr = __ldg(p.st.groups + g);  // dx, dz, lowest dy, (slots << 16) | first slot
     const int cnt = gr.w >> 16, pos = gr.w & 0xffff, wd = pos >> 5, sh = pos & 31;
@@ -69,6 +144,7 @@ __global__ void __launch_bounds__(kBondThreads, 2) k_deformation_tiled(const __g
     for (int q = 0; q < kTileP; ++q) {
       const uint32_t m = vp[q] ? group_bits(__ldg(p.st.mask + (int64_t)wd * n + ip[q]), sh, cm) : 0u;
       bits[q] = m << q;  // bit t: the neighbour at window position t (slot pos + t - q)
+      live[q] = 0u;
       if (DAMAGE) {
         const uint32_t bk = vp[q] ? group_bits(p.st.broken[(int64_t)wd * n + ip[q]], sh, cm) : 0u;
         live[q] = (m & fw & ~bk) << q;
@@ -77,7 +153,7 @@ __global__ void __launch_bounds__(kBondThreads, 2) k_deformation_tiled(const __g
     }
     if (__all_sync(0xffffffffu, any == 0u))
       continue;
-    const float gx = (float)gr.x * h, gz = (float)gr.y * h;
+    const float gx = (float)gr.x * h, gz = (float)gr.y * h, by0 = (float)gr.z * h;
     const int64_t jb = ((int64_t)(x + gr.x) * ny + (yb * kTileP + gr.z)) * nz + (z + gr.y);
     float part[kTileP][9];
 #pragma unroll
@@ -89,40 +165,26 @@ __global__ void __launch_bounds__(kBondThreads, 2) k_deformation_tiled(const __g
 #pragma unroll
     for (int q = 0; q < kTileP; ++q)
       fresh[q] = 0u, near[q] = 0u;
-    const int T = cnt + kTileP - 1;
-    for (int t = 0; t < T; ++t) {
-      const int64_t j = clamp_index(jb + (int64_t)t * nz, n);
-      const float4 a = ldgf4(p.jit + j), b = ldgf4(p.uf + j);
-      const float bx = a.x + gx, by = a.y + (float)(gr.z + t) * h, bz = a.z + gz;
-#pragma unroll
-      for (int q = 0; q < kTileP; ++q) {
-        if (t < q || t - q >= cnt)  // window position t holds no slot of point q (uniform)
-          continue;
-        const float e0 = bx - jx[q], e1 = by - jy[q], e2 = bz - jz[q];
-        const float d0 = b.x - ux[q], d1 = b.y - uy[q], d2 = b.z - uz[q];
-        const float v = ((bits[q] >> t) & 1u) ? a.w : 0.0f;  // no bond: no contribution
-        const float w0 = v * d0, w1 = v * d1, w2 = v * d2;
-        part[q][0] += w0 * e0, part[q][1] += w0 * e1, part[q][2] += w0 * e2;
-        part[q][3] += w1 * e0, part[q][4] += w1 * e1, part[q][5] += w1 * e2;
-        part[q][6] += w2 * e0, part[q][7] += w2 * e1, part[q][8] += w2 * e2;
-        if (DAMAGE && ((live[q] >> t) & 1u)) {
-          const float y0 = e0 + d0, y1 = e1 + d1, y2 = e2 + d2;
-          const float yy = y0 * y0 + y1 * y1 + y2 * y2;
-          const float xx = e0 * e0 + e1 * e1 + e2 * e2;
-          const float tt = p.tension2f * xx;
-          if (yy > tt * hi)
-            fresh[q] |= 1u << t;
-          else if (yy >= tt * lo)
-            near[q] |= 1u << t;
-          else if (p.use_compression) {
-            const float c = p.compression2f * xx;
-            if (yy < c * lo)
-              fresh[q] |= 1u << t;
-            else if (yy <= c * hi)
-              near[q] |= 1u << t;
-          }
-        }
+    if (UNROLL) {
+      static_assert(kUnrolledSlots == 12, "the cases below list the unrolled slot counts");
+      const int jb32 = (int)jb, nz32 = nz, n32 = (int)n;
+#define VPD_DEFORM_CASE(C)                                                                                \
+  case C:                                                                                                 \
+    deform_window<C, DAMAGE, kTileP, int>(p, cnt, jb32, nz32, n32, gx, gz, by0, h, pt, bits, live, part, \
+                                          fresh, near);                                                   \
+    break;
+      switch (cnt) {
+        VPD_DEFORM_CASE(1) VPD_DEFORM_CASE(2) VPD_DEFORM_CASE(3) VPD_DEFORM_CASE(4)
+        VPD_DEFORM_CASE(5) VPD_DEFORM_CASE(6) VPD_DEFORM_CASE(7) VPD_DEFORM_CASE(8)
+        VPD_DEFORM_CASE(9) VPD_DEFORM_CASE(10) VPD_DEFORM_CASE(11) VPD_DEFORM_CASE(12)
+      default:
+        deform_window<0, DAMAGE, kTileP, int>(p, cnt, jb32, nz32, n32, gx, gz, by0, h, pt, bits, live, part,
+                                              fresh, near);
       }
+#undef VPD_DEFORM_CASE
+    } else {
+      deform_window<0, DAMAGE, kTileP, int64_t>(p, cnt, jb, (int64_t)nz, n, gx, gz, by0, h, pt, bits, live,
+                                                part, fresh, near);
     }
 #pragma unroll
     for (int q = 0; q < kTileP; ++q)
@@ -162,8 +224,46 @@ __global__ void __launch_bounds__(kBondThreads, 2) k_deformation_tiled(const __g
         p.Gf[c * n + ip[q]] = G[q][c];
 }
 
+// ------------------------------------------------------------------ force
+template <int P> struct ForcePoints {
+  float jx[P], jy[P], jz[P];
+};
+
+template <int P, typename I>
+__device__ __forceinline__ void force_element(const StepParams &p, int t, int cnt, I j, float gx, float gz,
+                                              float by0, float h, const ForcePoints<P> &pt,
+                                              const uint32_t (&bits)[P], float (&part)[P][3]) {
+  const float4 a = ldgf4(p.fmapf + j), b = ldgf4(p.fmapf + p.n + j), c = ldgf4(p.fmapf + 2 * p.n + j);
+  const float bx = a.w + gx, by = b.w + fmaf((float)t, h, by0), bz = c.w + gz;
+#pragma unroll
+  for (int q = 0; q < P; ++q) {
+    if (t < q || t - q >= cnt)  // window position t holds no slot of point q
+      continue;
+    const bool bond = bits[q] & (1u << t);
+    const float e0 = bond ? bx - pt.jx[q] : 0.0f, e1 = bond ? by - pt.jy[q] : 0.0f;
+    const float e2 = bond ? bz - pt.jz[q] : 0.0f;
+    part[q][0] += a.x * e0 + a.y * e1 + a.z * e2;
+    part[q][1] += b.x * e0 + b.y * e1 + b.z * e2;
+    part[q][2] += c.x * e0 + c.y * e1 + c.z * e2;
+  }
+}
+
+template <int CNT, int P, typename I>
+__device__ __forceinline__ void force_window(const StepParams &p, int cnt, I jb, I nz, I n, float gx, float gz,
+                                             float by0, float h, const ForcePoints<P> &pt,
+                                             const uint32_t (&bits)[P], float (&part)[P][3]) {
+  if constexpr (CNT > 0) {
+#pragma unroll
+    for (int t = 0; t < CNT + P - 1; ++t)
+      force_element<P, I>(p, t, CNT, clamp_to<I>(jb + (I)t * nz, n), gx, gz, by0, h, pt, bits, part);
+  } else {
+    for (int t = 0; t < cnt + P - 1; ++t)
+      force_element<P, I>(p, t, cnt, clamp_to<I>(jb + (I)t * nz, n), gx, gz, by0, h, pt, bits, part);
+  }
+}
+
 // f = sum (V_j M_j) xi over intact bonds + M_i s_i with s_i = vxi_i - sum_{broken j} V_j xi.
-template <int kTileP>
+template <int kTileP, bool UNROLL>
 __global__ void __launch_bounds__(kBondThreads, 2) k_force_tiled(const __grid_constant__ StepParams p) {
   const int64_t n = p.n;
   const int ny = p.lat_ny, nz = p.lat_nz;
@@ -173,14 +273,14 @@ __global__ void __launch_bounds__(kBondThreads, 2) k_force_tiled(const __grid_co
   const float4 *P0 = p.fmapf, *P1 = p.fmapf + n, *P2 = p.fmapf + 2 * n;
   int64_t ip[kTileP];
   bool vp[kTileP];
-  float jx[kTileP], jy[kTileP], jz[kTileP];
+  ForcePoints<kTileP> pt;
 #pragma unroll
   for (int q = 0; q < kTileP; ++q) {
     const int y = yb * kTileP + q;
     vp[q] = inb && y < ny;
     ip[q] = vp[q] ? ((int64_t)x * ny + y) * nz + z : 0;
     const float4 a = ldgf4(p.jit + ip[q]);
-    jx[q] = a.x, jy[q] = a.y + (float)q * h, jz[q] = a.z;
+    pt.jx[q] = a.x, pt.jy[q] = a.y + (float)q * h, pt.jz[q] = a.z;
   }
   float fs[kTileP][3], fc[kTileP][3];
   double corr[kTileP][3];
@@ -215,28 +315,29 @@ __global__ void __launch_bounds__(kBondThreads, 2) k_force_tiled(const __grid_co
     }
     if (__all_sync(0xffffffffu, any == 0u))
       continue;
-    const float gx = (float)gr.x * h, gz = (float)gr.y * h;
+    const float gx = (float)gr.x * h, gz = (float)gr.y * h, by0 = (float)gr.z * h;
     const int64_t jb = ((int64_t)(x + gr.x) * ny + (yb * kTileP + gr.z)) * nz + (z + gr.y);
     float part[kTileP][3];
 #pragma unroll
     for (int q = 0; q < kTileP; ++q)
       part[q][0] = part[q][1] = part[q][2] = 0.0f;
-    const int T = cnt + kTileP - 1;
-    for (int t = 0; t < T; ++t) {
-      const int64_t j = clamp_index(jb + (int64_t)t * nz, n);
-      const float4 a = ldgf4(P0 + j), b = ldgf4(P1 + j), c = ldgf4(P2 + j);
-      const float bx = a.w + gx, by = b.w + (float)(gr.z + t) * h, bz = c.w + gz;
-#pragma unroll
-      for (int q = 0; q < kTileP; ++q) {
-        if (t < q || t - q >= cnt)  // window position t holds no slot of point q (uniform)
-          continue;
-        const bool bond = (bits[q] >> t) & 1u;
-        const float e0 = bond ? bx - jx[q] : 0.0f, e1 = bond ? by - jy[q] : 0.0f;
-        const float e2 = bond ? bz - jz[q] : 0.0f;
-        part[q][0] += a.x * e0 + a.y * e1 + a.z * e2;
-        part[q][1] += b.x * e0 + b.y * e1 + b.z * e2;
-        part[q][2] += c.x * e0 + c.y * e1 + c.z * e2;
+    if (UNROLL) {
+      static_assert(kUnrolledSlots == 12, "the cases below list the unrolled slot counts");
+      const int jb32 = (int)jb, nz32 = nz, n32 = (int)n;
+#define VPD_FORCE_CASE(C)                                                                               \
+  case C:                                                                                               \
+    force_window<C, kTileP, int>(p, cnt, jb32, nz32, n32, gx, gz, by0, h, pt, bits, part);             \
+    break;
+      switch (cnt) {
+        VPD_FORCE_CASE(1) VPD_FORCE_CASE(2) VPD_FORCE_CASE(3) VPD_FORCE_CASE(4)
+        VPD_FORCE_CASE(5) VPD_FORCE_CASE(6) VPD_FORCE_CASE(7) VPD_FORCE_CASE(8)
+        VPD_FORCE_CASE(9) VPD_FORCE_CASE(10) VPD_FORCE_CASE(11) VPD_FORCE_CASE(12)
+      default:
+        force_window<0, kTileP, int>(p, cnt, jb32, nz32, n32, gx, gz, by0, h, pt, bits, part);
       }
+#undef VPD_FORCE_CASE
+    } else {
+      force_window<0, kTileP, int64_t>(p, cnt, jb, (int64_t)nz, n, gx, gz, by0, h, pt, bits, part);
     }
 #pragma unroll
     for (int q = 0; q < kTileP; ++q)
@@ -260,33 +361,48 @@ __global__ void __launch_bounds__(kBondThreads, 2) k_force_tiled(const __grid_co
   }
 }
 
+// ------------------------------------------------------------------ launchers
 template <int kTileP> static unsigned tiled_grid(const StepParams &p) {
   const int64_t threads = (int64_t)p.lat_nx * ((p.lat_ny + kTileP - 1) / kTileP) * p.lat_nz;
   return (unsigned)((threads + kBondThreads - 1) / kBondThreads);
 }
 
+// 32-bit window indices need every index within a stencil reach of the lattice below 2^31
+static bool index32(const StepParams &p) { return p.n < (int64_t(1) << 30); }
+
+// With damage the deformation kernel keeps the runtime window loop: unrolled, the stretch
+// tests make it slower (0.28 against 0.25 ms on the 250k-point bar).
+template <int kTileP, bool UNROLL> static void launch_deformation(const StepParams &p, cudaStream_t s) {
+  if (p.damage)
+    k_deformation_tiled<true, kTileP, false><<<tiled_grid<kTileP>(p), kBondThreads, 0, s>>>(p);
+  else
+    k_deformation_tiled<false, kTileP, UNROLL><<<tiled_grid<kTileP>(p), kBondThreads, 0, s>>>(p);
+}
+
 // points per thread: 2 unless VPD_BOND_KERNEL=tiled3 (read when the handle is created)
 int launch_deformation_tiled(const StepParams &p, cudaStream_t s) {
-  if (p.tiled == 3) {
-    if (p.damage)
-      k_deformation_tiled<true, 3><<<tiled_grid<3>(p), kBondThreads, 0, s>>>(p);
-    else
-      k_deformation_tiled<false, 3><<<tiled_grid<3>(p), kBondThreads, 0, s>>>(p);
-  } else {
-    if (p.damage)
-      k_deformation_tiled<true, 2><<<tiled_grid<2>(p), kBondThreads, 0, s>>>(p);
-    else
-      k_deformation_tiled<false, 2><<<tiled_grid<2>(p), kBondThreads, 0, s>>>(p);
-  }
+  const bool u = index32(p);
+  if (p.tiled == 3)
+    u ? launch_deformation<3, true>(p, s) : launch_deformation<3, false>(p, s);
+  else
+    u ? launch_deformation<2, true>(p, s) : launch_deformation<2, false>(p, s);
   VPD_CUDA(cudaGetLastError());
   return VPD_OK;
 }
 
 int launch_force_tiled(const StepParams &p, cudaStream_t s) {
-  if (p.tiled == 3)
-    k_force_tiled<3><<<tiled_grid<3>(p), kBondThreads, 0, s>>>(p);
-  else
-    k_force_tiled<2><<<tiled_grid<2>(p), kBondThreads, 0, s>>>(p);
+  const bool u = index32(p);
+  if (p.tiled == 3) {
+    if (u)
+      k_force_tiled<3, true><<<tiled_grid<3>(p), kBondThreads, 0, s>>>(p);
+    else
+      k_force_tiled<3, false><<<tiled_grid<3>(p), kBondThreads, 0, s>>>(p);
+  } else {
+    if (u)
+      k_force_tiled<2, true><<<tiled_grid<2>(p), kBondThreads, 0, s>>>(p);
+    else
+      k_force_tiled<2, false><<<tiled_grid<2>(p), kBondThreads, 0, s>>>(p);
+  }
   VPD_CUDA(cudaGetLastError());
   return VPD_OK;
 }
