@@ -89,37 +89,71 @@ __global__ void __launch_bounds__(128, 1) k_mlp_forward(MlpWeights w, const floa
 //       Bt (Y_prev^T, 128x128) | small (dZ4^T 16x128) | barrier
 constexpr size_t kBwdSmem = 32768 * 2 + 4096 + 32768 * 3 + 4096 + 64;
 
-// Accumulates the calling thread's TMEM row of a weight-gradient product into grad[row][*].
-__device__ __forceinline__ void flush_grad(uint32_t trow, int ncols, float *grad_row, int stride) {
-  for (int c0 = 0; c0 < ncols; c0 += 16) {
-    float v[16];
-    umma::tmem_ld16(trow + c0, v);
+// Column sums of a 16-column slab over the 32 lanes of a warp, by halving: each step a lane
+// keeps half of its columns and adds the partner's copy of them (16 shuffles in all). Lane l
+// returns the sum of column col = 8 b4 + 4 b3 + 2 b2 + b1 (b_k: bit k of l); lanes l and l ^ 1
+// hold the same column.
+__device__ __forceinline__ float warp_column_sums16(const float (&v)[16], int lane, int &col) {
+  const bool h4 = lane & 16, h3 = lane & 8, h2 = lane & 4, h1 = lane & 2;
+  float a[8], b[4], d[2];
 #pragma unroll
-    for (int c = 0; c < 16; ++c)
-      if (c0 + c < ncols)
-        atomicAdd(grad_row + (size_t)(c0 + c) * stride, v[c]);
+  for (int c = 0; c < 8; ++c)
+    a[c] = (h4 ? v[c + 8] : v[c]) + __shfl_xor_sync(0xffffffffu, h4 ? v[c] : v[c + 8], 16);
+#pragma unroll
+  for (int c = 0; c < 4; ++c)
+    b[c] = (h3 ? a[c + 4] : a[c]) + __shfl_xor_sync(0xffffffffu, h3 ? a[c] : a[c + 4], 8);
+#pragma unroll
+  for (int c = 0; c < 2; ++c)
+    d[c] = (h2 ? b[c + 2] : b[c]) + __shfl_xor_sync(0xffffffffu, h2 ? b[c] : b[c + 2], 4);
+  float e = (h1 ? d[1] : d[0]) + __shfl_xor_sync(0xffffffffu, h1 ? d[0] : d[1], 2);
+  e += __shfl_xor_sync(0xffffffffu, e, 1);
+  col = (h4 ? 8 : 0) + (h3 ? 4 : 0) + (h2 ? 2 : 0) + (h1 ? 1 : 0);
+  return e;
+}
+
+// Thread t copies its batch row of a row-major bf16 matrix [rows][kin] into column t of a
+// K-major tile whose rows are the kin inputs (K = the 128 batch rows): 16-byte row loads,
+// and the 2-byte stores of a warp fall in four 16-byte runs.
+__device__ __forceinline__ void stage_row_as_column(unsigned char *tile, const __nv_bfloat16 *src, int64_t row,
+                                                    int64_t rows, int kin) {
+  const int t = threadIdx.x;
+  for (int c8 = 0; c8 < kin; c8 += 8) {
+    uint4 q = make_uint4(0u, 0u, 0u, 0u);
+    if (row < rows)
+      q = *reinterpret_cast<const uint4 *>(src + row * kin + c8);
+    const __nv_bfloat16 *e = reinterpret_cast<const __nv_bfloat16 *>(&q);
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+      *reinterpret_cast<__nv_bfloat16 *>(tile + kmajor_offset(c8 + j, t, 128)) = e[j];
   }
 }
 
-__global__ void __launch_bounds__(128, 1) k_mlp_backward(MlpWeights w, MlpActs acts, const float *gout,
-                                                         int64_t B, MlpGrads g, unsigned *err) {
+// One 128-row batch tile per block. The weight gradients of the tile (tensor-core products in
+// TMEM) and its bias gradients (warp column sums) are written to the block's slice of
+// `partials` [gridDim.x][kMlpParams]; k_sum_partials adds the slices in block order, so the
+// result does not depend on the order the blocks run in. wt holds W2^T, W3^T and W4^T
+// (row-major [in][out]), made once per pass by k_transpose_weights.
+__global__ void __launch_bounds__(128, 1) k_mlp_backward(MlpWeights w, const __nv_bfloat16 *wt, MlpActs acts,
+                                                         const float *gout, int64_t B, float *partials,
+                                                         unsigned *err) {
   extern __shared__ __align__(1024) unsigned char smem[];
   unsigned char *sWt2 = smem, *sWt3 = smem + 32768, *sWt4 = smem + 65536;
   unsigned char *sA = sWt4 + 4096, *sAt = sA + 32768, *sBt = sAt + 32768, *sSm = sBt + 32768;
   uint64_t *mbar = reinterpret_cast<uint64_t *>(sSm + 4096);
   __shared__ uint32_t s_tmem;
-  __shared__ float s_db[kMlpHidden];
-  const int t = threadIdx.x;
+  __shared__ float s_db[4][kMlpHidden];
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   const int64_t row0 = (int64_t)blockIdx.x * 128, row = row0 + t;
   const bool keep = row < B;
+  const MlpGrads g = mlp_grads(partials + (size_t)blockIdx.x * kMlpParams);
   if (t < 32)
     umma::tmem_alloc(&s_tmem, 256);
   if (t == 0)
     umma::mbar_init(mbar, 1);
   // transposed weights: B operand rows = layer inputs, K = layer outputs
-  stage_transposed(sWt2, w.w2, kMlpHidden, kMlpHidden);
-  stage_transposed(sWt3, w.w3, kMlpHidden, kMlpHidden);
-  stage_transposed(sWt4, w.w4, kMlpOut, kMlpHidden);
+  stage_rowmajor(sWt2, wt, kMlpHidden, kMlpHidden);
+  stage_rowmajor(sWt3, wt + 16384, kMlpHidden, kMlpHidden);
+  stage_rowmajor(sWt4, wt + 32768, kMlpHidden, kMlpOut);
   umma::fence_before_sync();
   __syncthreads();
   umma::fence_after_sync();
@@ -137,19 +171,21 @@ __global__ void __launch_bounds__(128, 1) k_mlp_backward(MlpWeights w, MlpActs a
   for (int c = 0; c < kMlpOut; ++c) {
     st_bf16(sA, t, c, kMlpOut, dz4[c]);          // A for dY3: rows x K=16
     st_bf16(sSm, c, t, 128, dz4[c]);             // B for dW4^T: N=16 rows x K=128 rows
-    atomicAdd(g.b4 + c, dz4[c]);
   }
-  // Y3^T into Bt (rows = 128 inputs, K = batch rows)
-  for (int e = t; e < 128 * kMlpHidden; e += 128) {
-    const int r = e / kMlpHidden, c = e % kMlpHidden;
-    const __nv_bfloat16 y = row0 + r < B ? acts.y3[(row0 + r) * kMlpHidden + c] : __float2bfloat16(0.0f);
-    *reinterpret_cast<__nv_bfloat16 *>(sBt + kmajor_offset(c, r, 128)) = y;
+  {
+    int col;
+    const float sum = warp_column_sums16(dz4, lane, col);
+    if (!(lane & 1))
+      s_db[warp][col] = sum;
   }
+  stage_row_as_column(sBt, acts.y3, row, B, kMlpHidden);  // Y3^T (rows = 128 inputs, K = batch rows)
   // dW4^T [in][out] = Y3^T dZ4 ; dY3 = dZ4 W4
   umma::fence_proxy_async();
   umma::fence_before_sync();
   __syncthreads();
   umma::fence_after_sync();
+  if (t < kMlpOut)
+    g.b4[t] = s_db[0][t] + s_db[1][t] + s_db[2][t] + s_db[3][t];
   if (t == 0) {
     umma::gemm_issue(tmem + 128, smem_u32(sBt), smem_u32(sSm), 128, kMlpOut, false);
     umma::gemm_issue(tmem, smem_u32(sA), smem_u32(sWt4), kMlpOut, kMlpHidden, false);
@@ -162,7 +198,7 @@ __global__ void __launch_bounds__(128, 1) k_mlp_backward(MlpWeights w, MlpActs a
     umma::tmem_ld16(tdw, v);
 #pragma unroll
     for (int c = 0; c < kMlpOut; ++c)
-      atomicAdd(g.w4 + (size_t)c * kMlpHidden + t, v[c]);
+      g.w4[(size_t)c * kMlpHidden + t] = v[c];
   }
 
   // ---- hidden layers 3, 2, 1
@@ -173,32 +209,31 @@ __global__ void __launch_bounds__(128, 1) k_mlp_backward(MlpWeights w, MlpActs a
     float *gw = layer == 3 ? g.w3 : (layer == 2 ? g.w2 : g.w1);
     float *gb = layer == 3 ? g.b3 : (layer == 2 ? g.b2 : g.b1);
     // dZ = dY * SiLU'(Z): this thread's row of dY from TMEM
-    if (t < kMlpHidden)
-      s_db[t] = 0.0f;
-    __syncthreads();
     for (int c0 = 0; c0 < kMlpHidden; c0 += 16) {
       float v[16];
       umma::tmem_ld16(tdy + c0, v);
+      __align__(16) __nv_bfloat16 zb[16];
 #pragma unroll
       for (int c = 0; c < 16; ++c) {
-        const float dz = keep ? v[c] * silu_grad(z[row * kMlpHidden + c0 + c]) : 0.0f;
-        st_bf16(sA, t, c0 + c, kMlpHidden, dz);   // A for dY_prev: rows x K=128 outputs
-        st_bf16(sAt, c0 + c, t, 128, dz);         // A for dW: outputs x K=128 rows
-        atomicAdd(&s_db[c0 + c], dz);
+        v[c] = keep ? v[c] * silu_grad(z[row * kMlpHidden + c0 + c]) : 0.0f;
+        zb[c] = __float2bfloat16(v[c]);
+        *reinterpret_cast<__nv_bfloat16 *>(sAt + kmajor_offset(c0 + c, t, 128)) = zb[c];  // dW's A
       }
+      // A for dY_prev: rows x K=128 outputs, two 16-byte rows of core matrices
+      *reinterpret_cast<uint4 *>(sA + kmajor_offset(t, c0, kMlpHidden)) = *reinterpret_cast<const uint4 *>(zb);
+      *reinterpret_cast<uint4 *>(sA + kmajor_offset(t, c0 + 8, kMlpHidden)) =
+          *reinterpret_cast<const uint4 *>(zb + 8);
+      int col;
+      const float sum = warp_column_sums16(v, lane, col);
+      if (!(lane & 1))
+        s_db[warp][c0 + col] = sum;
     }
-    // Y_prev^T into Bt (rows = inputs, K = batch rows)
-    for (int e = t; e < 128 * kin; e += 128) {
-      const int r = e / kin, c = e % kin;
-      const __nv_bfloat16 y = row0 + r < B ? yprev[(row0 + r) * kin + c] : __float2bfloat16(0.0f);
-      *reinterpret_cast<__nv_bfloat16 *>(sBt + kmajor_offset(c, r, 128)) = y;
-    }
+    stage_row_as_column(sBt, yprev, row, B, kin);  // Y_prev^T (rows = inputs, K = batch rows)
     umma::fence_proxy_async();
     umma::fence_before_sync();
     __syncthreads();
     umma::fence_after_sync();
-    if (t < kMlpHidden)
-      atomicAdd(gb + t, s_db[t]);
+    gb[t] = s_db[0][t] + s_db[1][t] + s_db[2][t] + s_db[3][t];
     if (t == 0) {
       umma::gemm_issue(tmem + 128, smem_u32(sAt), smem_u32(sBt), 128, kin, false);  // dW [out][in]
       if (layer > 1)
@@ -208,12 +243,42 @@ __global__ void __launch_bounds__(128, 1) k_mlp_backward(MlpWeights w, MlpActs a
     }
     sy.wait();
     if (sy.ok)
-      flush_grad(tdw, kin, gw + (size_t)t * kin, 1);
+      for (int c0 = 0; c0 < kin; c0 += 16) {  // this thread's row of dW [out][in]
+        float v[16];
+        umma::tmem_ld16(tdw + c0, v);
+        float4 *dst = reinterpret_cast<float4 *>(gw + (size_t)t * kin + c0);
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          dst[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+      }
   }
   umma::fence_before_sync();
   __syncthreads();
   if (t < 32)
     umma::tmem_dealloc(tmem, 256);
+}
+
+// W2^T, W3^T and W4^T (row-major [in][out]) for the backward pass's B operands.
+__global__ void k_transpose_weights(MlpWeights w, __nv_bfloat16 *wt) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e < 2 * 16384) {
+    const int l = e >> 14, r = (e >> 7) & 127, c = e & 127;  // wt[l][r = in][c = out]
+    wt[e] = (l ? w.w3 : w.w2)[c * 128 + r];
+  } else if (e < 2 * 16384 + 2048) {
+    const int f = e - 2 * 16384, r = f >> 4, c = f & 15;  // [in 128][out 16]
+    wt[e] = w.w4[c * 128 + r];
+  }
+}
+
+// grad[i] = sum over blocks b (in order) of partials[b][i].
+__global__ void k_sum_partials(const float *partials, int nblocks, float *grad) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= kMlpParams)
+    return;
+  float s = 0.0f;
+  for (int b = 0; b < nblocks; ++b)
+    s += partials[(size_t)b * kMlpParams + i];
+  grad[i] = s;
 }
 
 // ------------------------------------------------------------------ Adam and helpers
@@ -264,9 +329,16 @@ int mlp_forward(const MlpWeights &w, const float *x, int64_t B, float *out, cons
   return VPD_OK;
 }
 
-int mlp_backward(const MlpWeights &w, const MlpActs &acts, const float *gout, int64_t B, const MlpGrads &g,
-                 unsigned *err, cudaStream_t s) {
-  k_mlp_backward<<<(unsigned)((B + 127) / 128), 128, kBwdSmem, s>>>(w, acts, gout, B, g, err);
+int64_t mlp_backward_blocks(int64_t B) { return (B + 127) / 128; }
+
+int mlp_backward(const MlpWeights &w, const MlpActs &acts, const float *gout, int64_t B, float *grad,
+                 const MlpBackwardScratch &scr, unsigned *err, cudaStream_t s) {
+  const int64_t nb = mlp_backward_blocks(B);
+  k_transpose_weights<<<(2 * 16384 + 2048 + 255) / 256, 256, 0, s>>>(w, scr.wt);
+  VPD_CUDA(cudaGetLastError());
+  k_mlp_backward<<<(unsigned)nb, 128, kBwdSmem, s>>>(w, scr.wt, acts, gout, B, scr.partials, err);
+  VPD_CUDA(cudaGetLastError());
+  k_sum_partials<<<(unsigned)((kMlpParams + 255) / 256), 256, 0, s>>>(scr.partials, (int)nb, grad);
   VPD_CUDA(cudaGetLastError());
   return VPD_OK;
 }
@@ -327,7 +399,9 @@ extern "C" int vpd_mlp_gradients(const uint16_t *weights, const float *biases, c
   const MlpWeights w = mlp_weights(reinterpret_cast<const __nv_bfloat16 *>(weights), biases);
   unsigned char *buf = nullptr;
   const size_t nb = (size_t)batch;
-  const size_t bytes = nb * kMlpIn * 2 + nb * kMlpHidden * (4 * 3 + 2 * 3) + nb * kMlpOut * 4 + 256;
+  const size_t blocks = (size_t)mlp_backward_blocks(batch);
+  const size_t bytes = nb * kMlpIn * 2 + nb * kMlpHidden * (4 * 3 + 2 * 3) + nb * kMlpOut * 4 + 256 +
+                       sizeof(float) * blocks * kMlpParams + sizeof(uint16_t) * kMlpWeights;
   VPD_CUDA(cudaMalloc(&buf, bytes));
   MlpActs a;
   unsigned char *q = buf;
@@ -340,6 +414,10 @@ extern "C" int vpd_mlp_gradients(const uint16_t *weights, const float *biases, c
   a.y3 = reinterpret_cast<__nv_bfloat16 *>(q), q += nb * kMlpHidden * 2;
   float *out = reinterpret_cast<float *>(q), *derrf = out + nb * kMlpOut;
   unsigned *derr = reinterpret_cast<unsigned *>(derrf);
+  q = reinterpret_cast<unsigned char *>(derrf) + 256;
+  MlpBackwardScratch scr;
+  scr.partials = reinterpret_cast<float *>(q), q += sizeof(float) * blocks * kMlpParams;
+  scr.wt = reinterpret_cast<__nv_bfloat16 *>(q);
   int rc = VPD_OK;
   cudaError_t e = cudaMemsetAsync(derr, 0, sizeof(unsigned), s);
   if (e == cudaSuccess)
@@ -349,7 +427,7 @@ extern "C" int vpd_mlp_gradients(const uint16_t *weights, const float *biases, c
   if (rc == VPD_OK)
     rc = mlp_forward(w, x, batch, out, a, derr, s);
   if (rc == VPD_OK)
-    rc = mlp_backward(w, a, gout, batch, mlp_grads(grad), derr, s);
+    rc = mlp_backward(w, a, gout, batch, grad, scr, derr, s);
   if (rc == VPD_OK)
     rc = check_err(derr, s);
   cudaFree(buf);

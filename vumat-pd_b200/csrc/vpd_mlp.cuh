@@ -44,8 +44,16 @@ __host__ __device__ inline MlpGrads mlp_grads(float *g) {
 
 int mlp_forward(const MlpWeights &w, const float *x, int64_t B, float *out, const MlpActs &acts,
                 unsigned *err, cudaStream_t s);
-int mlp_backward(const MlpWeights &w, const MlpActs &acts, const float *gout, int64_t B,
-                 const MlpGrads &g, unsigned *err, cudaStream_t s);
+// Scratch of one backward pass: the transposed weights (VPD_MLP_WEIGHTS - 2048 bf16) and one
+// partial gradient per 128-row block (mlp_backward_blocks(B) x kMlpParams floats).
+struct MlpBackwardScratch {
+  __nv_bfloat16 *wt;
+  float *partials;
+};
+int64_t mlp_backward_blocks(int64_t B);
+// grad [kMlpParams] = d/dparams of sum(out * gout) over the batch (overwritten, not accumulated).
+int mlp_backward(const MlpWeights &w, const MlpActs &acts, const float *gout, int64_t B, float *grad,
+                 const MlpBackwardScratch &scr, unsigned *err, cudaStream_t s);
 int mlp_adam(float *p, float *m, float *v, float *grad, __nv_bfloat16 *pb, int64_t n, float lr,
              int step, cudaStream_t s);
 int mlp_mse_grad(const float *out, const float *target, int64_t B, int cols, float *gout,

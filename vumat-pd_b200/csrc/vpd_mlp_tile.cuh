@@ -46,15 +46,6 @@ __device__ __forceinline__ void stage_rowmajor(unsigned char *tile, const __nv_b
   }
 }
 
-// Copies the transpose of a row-major bf16 matrix [rows][cols] into a K-major tile whose rows
-// are the source columns (K = rows).
-__device__ __forceinline__ void stage_transposed(unsigned char *tile, const __nv_bfloat16 *src, int rows, int cols) {
-  for (int e = threadIdx.x; e < rows * cols; e += blockDim.x) {
-    const int r = e / cols, c = e % cols;
-    *reinterpret_cast<__nv_bfloat16 *>(tile + kmajor_offset(c, r, rows)) = src[(size_t)r * cols + c];
-  }
-}
-
 struct Sync {
   uint64_t *mbar;
   uint32_t phase;

@@ -275,6 +275,10 @@ int train_surrogate(const vpd_surrogate_config &cfg, uint16_t *w_out, float *b_o
       (rc = buf.alloc(&loss, VPD_SURROGATE_MAX_EPOCHS + 1)) || (rc = buf.alloc(&vout, VB * 16)) ||
       (rc = buf.alloc(&err, 1)))
     return rc;
+  MlpBackwardScratch bscr{};
+  if ((rc = buf.alloc(&bscr.wt, kMlpWeights)) ||
+      (rc = buf.alloc(&bscr.partials, (size_t)mlp_backward_blocks(B) * kMlpParams)))
+    return rc;
   if ((rc = surrogate_samples_dev(jc, cfg.seed, S, X, Y, nullptr, s)))
     return rc;
 
@@ -307,7 +311,6 @@ int train_surrogate(const vpd_surrogate_config &cfg, uint16_t *w_out, float *b_o
 
   const MlpWeights w = mlp_weights(Wb, P + kMlpWeights);
   const MlpActs acts{y0, z1, z2, z3, y1, y2, y3};
-  const MlpGrads grads = mlp_grads(G);
   const int64_t steps = T / B;
   int adam_step = 0;
   VPD_CUDA(cudaEventRecord(g.e0, s));
@@ -320,7 +323,7 @@ int train_surrogate(const vpd_surrogate_config &cfg, uint16_t *w_out, float *b_o
         return rc;
       k_weighted_mse<<<(unsigned)((B + 255) / 256), 256, 0, s>>>(out, Yb, B, gout, loss + e);
       VPD_CUDA(cudaGetLastError());
-      if ((rc = mlp_backward(w, acts, gout, B, grads, err, s)))
+      if ((rc = mlp_backward(w, acts, gout, B, G, bscr, err, s)))
         return rc;
       ++adam_step;
       if ((rc = mlp_adam(P, M, Vm, G, Wb, kMlpWeights, (float)cfg.learning_rate, adam_step, s)) ||
