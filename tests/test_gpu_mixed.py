@@ -66,10 +66,10 @@ def test_mixed_requires_lattice_layout(monkeypatch):
 
 @pytest.mark.parametrize("damage", [0, 1])
 def test_tiled_bond_kernels_match_slot_kernels(monkeypatch, damage):
-    """The tiled bond kernels (points per thread along y, one load per neighbour record per
-    stencil group) against the per-slot kernels on the jittered horizon-4 bar: the same FP32
-    bond terms summed in another order, so the histories agree to FP32 rounding and the
-    bond-breaking decisions agree. With damage the comparison covers the early increments:
+    """The tiled bond kernels (two points per thread along y, one load per neighbour record
+    per stencil group; scalar FP32 and packed FP32 pairs) against the per-slot kernels on the
+    jittered horizon-4 bar: the same FP32 bond terms summed in another order, so the histories
+    agree to FP32 rounding and the bond-breaking decisions agree. With damage the comparison covers the early increments:
     later, rounding-level differences flip bonds at the threshold and the fracture paths part
     (as between the FP64 and mixed paths)."""
     case = tensile_bar(3, nx=24, ny=20, nz=17, damage_mode=damage, damage_initiation=0.004,
@@ -77,7 +77,7 @@ def test_tiled_bond_kernels_match_slot_kernels(monkeypatch, damage):
     steps = 120 if damage else 400
     monkeypatch.setenv("VPD_BOND_KERNEL", "slot")
     rs, us, es, ds = run(case, steps)
-    for kind in ("tiled2", "tiled3"):
+    for kind in ("scalar", "pair"):
         monkeypatch.setenv("VPD_BOND_KERNEL", kind)
         rt, ut, et, dt_ = run(case, steps)
         assert nrmse(rt[:, STRESS], rs[:, STRESS]) < 1e-5

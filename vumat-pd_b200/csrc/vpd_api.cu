@@ -422,11 +422,11 @@ int create_impl(vpd_handle *h, const vpd_case *c, const double *positions, const
   p.st = h->st;
   p.lat_nx = c->nx, p.lat_ny = c->ny, p.lat_nz = c->nz, p.lat_h = c->spacing;
   {
-    // VPD_BOND_KERNEL=slot selects the per-slot mixed-precision bond kernels, tiled3 the
-    // tiled kernels with three points per thread (default: two)
+    // VPD_BOND_KERNEL=slot selects the per-slot mixed-precision bond kernels, scalar the
+    // two-point tiled kernels in scalar FP32 (default: the packed-pair tiled kernels)
     const char *bk = getenv("VPD_BOND_KERNEL");
     const std::string kind = bk ? bk : "";
-    p.tiled = kind == "slot" ? 0 : (kind == "tiled3" ? 3 : 2);
+    p.tiled = kind == "slot" ? 0 : (kind == "scalar" ? 1 : 2);
   }
   if (p.st.nw && ((rc = dalloc(h, &p.vxi, n)) ||
                   (c->precision != VPD_PRECISION_MIXED && (rc = dalloc(h, &p.fmap, 3 * n)))))

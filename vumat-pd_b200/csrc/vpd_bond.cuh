@@ -19,6 +19,19 @@ __device__ __forceinline__ void kahan_add(float &s, float &c, float x) {
   s = t;
 }
 
+// Packed FP32 pairs: one sm_100a paired instruction (FADD2, FMUL2, FFMA2) applies the same
+// operation to both lanes, each lane rounded as the scalar operation.
+__device__ __forceinline__ float2 bcast2(float v) { return make_float2(v, v); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) {  // a - b: b (-1) is exact, one rounding
+  return __ffma2_rn(b, make_float2(-1.0f, -1.0f), a);
+}
+__device__ __forceinline__ void kahan_add2(float2 &s, float2 &c, float2 x) {  // kahan_add on each lane
+  const float2 y = sub2(x, c);
+  const float2 t = __fadd2_rn(s, y);
+  c = sub2(sub2(t, s), y);
+  s = t;
+}
+
 static __device__ __noinline__ bool exact_break_mixed(const double4 *xv, const double4 *U, int64_t i,
                                                int64_t j, double initiation, double failure,
                                                int use_compression) {

@@ -45,6 +45,55 @@ __device__ __forceinline__ uint32_t group_bits(uint32_t word, int shift, uint32_
 
 template <typename I> __device__ __forceinline__ I clamp_to(I j, I n) { return j < 0 ? 0 : (j >= n ? n - 1 : j); }
 
+// FP32 critical-stretch test of one live bond (reference xi = e, displacement difference d):
+// bit t of `fresh` when the bond is clearly broken, of `near` when it is within the 1e-5 margin
+// of a threshold and the exact FP64 test decides.
+__device__ __forceinline__ void stretch_test(const StepParams &p, int t, float e0, float e1, float e2, float d0,
+                                             float d1, float d2, uint32_t &fresh, uint32_t &near) {
+  const float lo = 1.0f - 1.0e-5f, hi = 1.0f + 1.0e-5f;
+  const float y0 = e0 + d0, y1 = e1 + d1, y2 = e2 + d2;
+  const float yy = y0 * y0 + y1 * y1 + y2 * y2;
+  const float xx = e0 * e0 + e1 * e1 + e2 * e2;
+  const float tt = p.tension2f * xx;
+  if (yy > tt * hi)
+    fresh |= 1u << t;
+  else if (yy >= tt * lo)
+    near |= 1u << t;
+  else if (p.use_compression) {
+    const float c = p.compression2f * xx;
+    if (yy < c * lo)
+      fresh |= 1u << t;
+    else if (yy <= c * hi)
+      near |= 1u << t;
+  }
+}
+
+// Point i's bonds of one group (first slot pos, mask word wd, shift sh) that the stretch tests
+// flagged: `near` ones decided by the exact FP64 test, then both directed bonds of every
+// broken pair marked (bit k: slot pos + k).
+__device__ __forceinline__ void commit_breaks(const StepParams &p, int64_t i, int pos, int wd, int sh, uint32_t fr,
+                                              uint32_t nr) {
+  const int64_t n = p.n;
+  if (nr) {
+    const int64_t step = *p.step;
+    const double4 *U = (step & 1) ? p.u1 : p.u0;
+    for (uint32_t f = nr; f; f &= f - 1) {
+      const int k = __ffs(f) - 1;
+      if (exact_break_mixed(p.xv, U, i, i + p.st.delta[pos + k], p.dmg_initiation, p.dmg_failure,
+                            p.use_compression))
+        fr |= 1u << k;
+    }
+  }
+  if (fr) {
+    atomicOr(p.st.broken + (int64_t)wd * n + i, fr << sh);
+    for (uint32_t f = fr; f; f &= f - 1) {
+      const int sl = pos + __ffs(f) - 1;
+      const int r = p.st.reverse[sl];
+      atomicOr(p.st.broken + (int64_t)(r >> 5) * n + (i + p.st.delta[sl]), 1u << (r & 31));
+    }
+  }
+}
+
 // ------------------------------------------------------------------ deformation
 template <int P> struct DeformPoints {
   float jx[P], jy[P], jz[P], ux[P], uy[P], uz[P];  // jy includes q h (y relative to the tile's base row)
@@ -58,7 +107,6 @@ __device__ __forceinline__ void deform_element(const StepParams &p, int t, int c
                                                float (&part)[P][9], uint32_t (&fresh)[P], uint32_t (&near)[P]) {
   const float4 a = ldgf4(p.jit + j), b = ldgf4(p.uf + j);
   const float bx = a.x + gx, by = a.y + fmaf((float)t, h, by0), bz = a.z + gz;
-  const float lo = 1.0f - 1.0e-5f, hi = 1.0f + 1.0e-5f;
 #pragma unroll
   for (int q = 0; q < P; ++q) {
     if (t < q || t - q >= cnt)  // window position t holds no slot of point q
@@ -70,23 +118,8 @@ __device__ __forceinline__ void deform_element(const StepParams &p, int t, int c
     part[q][0] += w0 * e0, part[q][1] += w0 * e1, part[q][2] += w0 * e2;
     part[q][3] += w1 * e0, part[q][4] += w1 * e1, part[q][5] += w1 * e2;
     part[q][6] += w2 * e0, part[q][7] += w2 * e1, part[q][8] += w2 * e2;
-    if (DAMAGE && (live[q] & (1u << t))) {
-      const float y0 = e0 + d0, y1 = e1 + d1, y2 = e2 + d2;
-      const float yy = y0 * y0 + y1 * y1 + y2 * y2;
-      const float xx = e0 * e0 + e1 * e1 + e2 * e2;
-      const float tt = p.tension2f * xx;
-      if (yy > tt * hi)
-        fresh[q] |= 1u << t;
-      else if (yy >= tt * lo)
-        near[q] |= 1u << t;
-      else if (p.use_compression) {
-        const float c = p.compression2f * xx;
-        if (yy < c * lo)
-          fresh[q] |= 1u << t;
-        else if (yy <= c * hi)
-          near[q] |= 1u << t;
-      }
-    }
+    if (DAMAGE && (live[q] & (1u << t)))
+      stretch_test(p, t, e0, e1, e2, d0, d1, d2, fresh[q], near[q]);
   }
 }
 
@@ -191,30 +224,10 @@ __global__ void __launch_bounds__(kBondThreads, 2) k_deformation_tiled(const __g
 #pragma unroll
       for (int c = 0; c < 9; ++c)
         G[q][c] += part[q][c];
-    if (DAMAGE) {
+    if (DAMAGE)
 #pragma unroll
-      for (int q = 0; q < kTileP; ++q) {
-        uint32_t fr = fresh[q] >> q;  // slot offsets within the group
-        if (near[q]) {
-          const int64_t step = *p.step;
-          const double4 *U = (step & 1) ? p.u1 : p.u0;
-          for (uint32_t f = near[q] >> q; f; f &= f - 1) {
-            const int k = __ffs(f) - 1;
-            if (exact_break_mixed(p.xv, U, ip[q], ip[q] + p.st.delta[pos + k], p.dmg_initiation,
-                                  p.dmg_failure, p.use_compression))
-              fr |= 1u << k;
-          }
-        }
-        if (fr) {
-          atomicOr(p.st.broken + (int64_t)wd * n + ip[q], fr << sh);
-          for (uint32_t f = fr; f; f &= f - 1) {
-            const int sl = pos + __ffs(f) - 1;
-            const int r = p.st.reverse[sl];
-            atomicOr(p.st.broken + (int64_t)(r >> 5) * n + (ip[q] + p.st.delta[sl]), 1u << (r & 31));
-          }
-        }
-      }
-    }
+      for (int q = 0; q < kTileP; ++q)  // window positions -> slot offsets within the group
+        commit_breaks(p, ip[q], pos, wd, sh, fresh[q] >> q, near[q] >> q);
   }
 #pragma unroll
   for (int q = 0; q < kTileP; ++q)
@@ -361,6 +374,274 @@ __global__ void __launch_bounds__(kBondThreads, 2) k_force_tiled(const __grid_co
   }
 }
 
+// ------------------------------------------------------------------ packed pairs
+// The default bond kernels: kTileP = 2 with the thread's two points held as the two lanes of
+// packed FP32 pairs, so each bond term of both points is one paired instruction (half the
+// arithmetic issue of the scalar kernels above). Windows, masks, operation order and rounding
+// per lane are those of the scalar kernels; a window position that holds a slot of only one
+// point (t = 0: point 0, t = cnt: point 1) runs with the other lane's bond weight zero.
+struct DeformPair {
+  float2 jx, jy, jz, ux, uy, uz;  // lane q: point q (jy includes q h)
+};
+
+template <bool DAMAGE, typename I>
+__device__ __forceinline__ void deform_pair_element(const StepParams &p, int t, I j, float gx, float gz, float by0,
+                                                    float h, const DeformPair &pt, const uint32_t (&bits)[2],
+                                                    const uint32_t (&live)[2], float2 (&part)[9],
+                                                    uint32_t (&fresh)[2], uint32_t (&near)[2]) {
+  const float4 a = ldgf4(p.jit + j), b = ldgf4(p.uf + j);
+  const float bx = a.x + gx, by = a.y + fmaf((float)t, h, by0), bz = a.z + gz;
+  const float2 e0 = sub2(bcast2(bx), pt.jx), e1 = sub2(bcast2(by), pt.jy), e2 = sub2(bcast2(bz), pt.jz);
+  const float2 d0 = sub2(bcast2(b.x), pt.ux), d1 = sub2(bcast2(b.y), pt.uy), d2 = sub2(bcast2(b.z), pt.uz);
+  // bit t of bits[q]: window position t is a bond of point q (clear where it holds no slot of q)
+  const float2 v = make_float2(((bits[0] >> t) & 1u) ? a.w : 0.0f, ((bits[1] >> t) & 1u) ? a.w : 0.0f);
+  const float2 w0 = __fmul2_rn(v, d0), w1 = __fmul2_rn(v, d1), w2 = __fmul2_rn(v, d2);
+  part[0] = __ffma2_rn(w0, e0, part[0]), part[1] = __ffma2_rn(w0, e1, part[1]);
+  part[2] = __ffma2_rn(w0, e2, part[2]), part[3] = __ffma2_rn(w1, e0, part[3]);
+  part[4] = __ffma2_rn(w1, e1, part[4]), part[5] = __ffma2_rn(w1, e2, part[5]);
+  part[6] = __ffma2_rn(w2, e0, part[6]), part[7] = __ffma2_rn(w2, e1, part[7]);
+  part[8] = __ffma2_rn(w2, e2, part[8]);
+  if (DAMAGE) {
+    if ((live[0] >> t) & 1u)
+      stretch_test(p, t, e0.x, e1.x, e2.x, d0.x, d1.x, d2.x, fresh[0], near[0]);
+    if ((live[1] >> t) & 1u)
+      stretch_test(p, t, e0.y, e1.y, e2.y, d0.y, d1.y, d2.y, fresh[1], near[1]);
+  }
+}
+
+template <int CNT, bool DAMAGE, typename I>
+__device__ __forceinline__ void deform_pair_window(const StepParams &p, int cnt, I jb, I nz, I n, float gx, float gz,
+                                                   float by0, float h, const DeformPair &pt,
+                                                   const uint32_t (&bits)[2], const uint32_t (&live)[2],
+                                                   float2 (&part)[9], uint32_t (&fresh)[2], uint32_t (&near)[2]) {
+  if constexpr (CNT > 0) {
+#pragma unroll
+    for (int t = 0; t < CNT + 1; ++t)
+      deform_pair_element<DAMAGE, I>(p, t, clamp_to<I>(jb + (I)t * nz, n), gx, gz, by0, h, pt, bits, live, part,
+                                     fresh, near);
+  } else {
+    for (int t = 0; t < cnt + 1; ++t)
+      deform_pair_element<DAMAGE, I>(p, t, clamp_to<I>(jb + (I)t * nz, n), gx, gz, by0, h, pt, bits, live, part,
+                                     fresh, near);
+  }
+}
+
+template <bool DAMAGE, bool UNROLL>
+__global__ void __launch_bounds__(kBondThreads, 2) k_deformation_pair(const __grid_constant__ StepParams p) {
+  const int64_t n = p.n;
+  const int ny = p.lat_ny, nz = p.lat_nz;
+  const float h = (float)p.lat_h;
+  int x, yb, z;
+  const bool inb = tile_coords<2>(p, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, x, yb, z);
+  int64_t ip[2];
+  bool vp[2];
+  float4 pa[2], pb[2];
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    const int y = yb * 2 + q;
+    vp[q] = inb && y < ny;
+    ip[q] = vp[q] ? ((int64_t)x * ny + y) * nz + z : 0;
+    pa[q] = ldgf4(p.jit + ip[q]), pb[q] = ldgf4(p.uf + ip[q]);
+  }
+  DeformPair pt;
+  pt.jx = make_float2(pa[0].x, pa[1].x), pt.jy = make_float2(pa[0].y, pa[1].y + h);
+  pt.jz = make_float2(pa[0].z, pa[1].z);
+  pt.ux = make_float2(pb[0].x, pb[1].x), pt.uy = make_float2(pb[0].y, pb[1].y);
+  pt.uz = make_float2(pb[0].z, pb[1].z);
+  float2 G[9];
+#pragma unroll
+  for (int c = 0; c < 9; ++c)
+    G[c] = make_float2(0.0f, 0.0f);
+  for (int g = 0; g < p.st.ngroups; ++g) {
+    const int4 gr = __ldg(p.st.groups + g);  // dx, dz, lowest dy, (slots << 16) | first slot
+    const int cnt = gr.w >> 16, pos = gr.w & 0xffff, wd = pos >> 5, sh = pos & 31;
+    const uint32_t cm = cnt >= 32 ? ~0u : ((1u << cnt) - 1u);
+    uint32_t bits[2], live[2];
+    const uint32_t fw = DAMAGE ? group_bits(__ldg(p.st.forward + wd), sh, cm) : 0u;
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const uint32_t m = vp[q] ? group_bits(__ldg(p.st.mask + (int64_t)wd * n + ip[q]), sh, cm) : 0u;
+      bits[q] = m << q;  // bit t: the neighbour at window position t (slot pos + t - q)
+      live[q] = 0u;
+      if (DAMAGE) {
+        const uint32_t bk = vp[q] ? group_bits(p.st.broken[(int64_t)wd * n + ip[q]], sh, cm) : 0u;
+        live[q] = (m & fw & ~bk) << q;
+      }
+    }
+    if (__all_sync(0xffffffffu, (bits[0] | bits[1]) == 0u))
+      continue;
+    const float gx = (float)gr.x * h, gz = (float)gr.y * h, by0 = (float)gr.z * h;
+    const int64_t jb = ((int64_t)(x + gr.x) * ny + (yb * 2 + gr.z)) * nz + (z + gr.y);
+    float2 part[9];
+#pragma unroll
+    for (int c = 0; c < 9; ++c)
+      part[c] = make_float2(0.0f, 0.0f);
+    uint32_t fresh[2] = {0u, 0u}, near[2] = {0u, 0u};
+    if (UNROLL) {
+      static_assert(kUnrolledSlots == 12, "the cases below list the unrolled slot counts");
+      const int jb32 = (int)jb, nz32 = nz, n32 = (int)n;
+#define VPD_DEFORM_CASE(C)                                                                                   \
+  case C:                                                                                                    \
+    deform_pair_window<C, DAMAGE, int>(p, cnt, jb32, nz32, n32, gx, gz, by0, h, pt, bits, live, part, fresh, \
+                                       near);                                                                \
+    break;
+      switch (cnt) {
+        VPD_DEFORM_CASE(1) VPD_DEFORM_CASE(2) VPD_DEFORM_CASE(3) VPD_DEFORM_CASE(4)
+        VPD_DEFORM_CASE(5) VPD_DEFORM_CASE(6) VPD_DEFORM_CASE(7) VPD_DEFORM_CASE(8)
+        VPD_DEFORM_CASE(9) VPD_DEFORM_CASE(10) VPD_DEFORM_CASE(11) VPD_DEFORM_CASE(12)
+      default:
+        deform_pair_window<0, DAMAGE, int>(p, cnt, jb32, nz32, n32, gx, gz, by0, h, pt, bits, live, part, fresh,
+                                           near);
+      }
+#undef VPD_DEFORM_CASE
+    } else {
+      deform_pair_window<0, DAMAGE, int64_t>(p, cnt, jb, (int64_t)nz, n, gx, gz, by0, h, pt, bits, live, part,
+                                             fresh, near);
+    }
+#pragma unroll
+    for (int c = 0; c < 9; ++c)
+      G[c] = __fadd2_rn(G[c], part[c]);
+    if (DAMAGE)
+#pragma unroll
+      for (int q = 0; q < 2; ++q)
+        commit_breaks(p, ip[q], pos, wd, sh, fresh[q] >> q, near[q] >> q);
+  }
+#pragma unroll
+  for (int c = 0; c < 9; ++c) {
+    if (vp[0])
+      p.Gf[c * n + ip[0]] = G[c].x;
+    if (vp[1])
+      p.Gf[c * n + ip[1]] = G[c].y;
+  }
+}
+
+struct ForcePair {
+  float2 jx, jy, jz;  // lane q: point q (jy includes q h)
+};
+
+template <typename I>
+__device__ __forceinline__ void force_pair_element(const StepParams &p, int t, I j, float gx, float gz, float by0,
+                                                   float h, const ForcePair &pt, const uint32_t (&bits)[2],
+                                                   float2 (&part)[3]) {
+  const float4 a = ldgf4(p.fmapf + j), b = ldgf4(p.fmapf + p.n + j), c = ldgf4(p.fmapf + 2 * p.n + j);
+  const float bx = a.w + gx, by = b.w + fmaf((float)t, h, by0), bz = c.w + gz;
+  const float2 e0 = sub2(bcast2(bx), pt.jx), e1 = sub2(bcast2(by), pt.jy), e2 = sub2(bcast2(bz), pt.jz);
+  // the row sums of V_j M_j xi, added to the lanes whose point has a bond at position t
+  const float2 m = make_float2(((bits[0] >> t) & 1u) ? 1.0f : 0.0f, ((bits[1] >> t) & 1u) ? 1.0f : 0.0f);
+  const float2 r0 = __ffma2_rn(bcast2(a.z), e2, __ffma2_rn(bcast2(a.y), e1, __fmul2_rn(bcast2(a.x), e0)));
+  const float2 r1 = __ffma2_rn(bcast2(b.z), e2, __ffma2_rn(bcast2(b.y), e1, __fmul2_rn(bcast2(b.x), e0)));
+  const float2 r2 = __ffma2_rn(bcast2(c.z), e2, __ffma2_rn(bcast2(c.y), e1, __fmul2_rn(bcast2(c.x), e0)));
+  part[0] = __ffma2_rn(m, r0, part[0]), part[1] = __ffma2_rn(m, r1, part[1]);
+  part[2] = __ffma2_rn(m, r2, part[2]);
+}
+
+template <int CNT, typename I>
+__device__ __forceinline__ void force_pair_window(const StepParams &p, int cnt, I jb, I nz, I n, float gx, float gz,
+                                                  float by0, float h, const ForcePair &pt, const uint32_t (&bits)[2],
+                                                  float2 (&part)[3]) {
+  if constexpr (CNT > 0) {
+#pragma unroll
+    for (int t = 0; t < CNT + 1; ++t)
+      force_pair_element<I>(p, t, clamp_to<I>(jb + (I)t * nz, n), gx, gz, by0, h, pt, bits, part);
+  } else {
+    for (int t = 0; t < cnt + 1; ++t)
+      force_pair_element<I>(p, t, clamp_to<I>(jb + (I)t * nz, n), gx, gz, by0, h, pt, bits, part);
+  }
+}
+
+// f = sum (V_j M_j) xi over intact bonds + M_i s_i with s_i = vxi_i - sum_{broken j} V_j xi.
+template <bool UNROLL>
+__global__ void __launch_bounds__(kBondThreads, 2) k_force_pair(const __grid_constant__ StepParams p) {
+  const int64_t n = p.n;
+  const int ny = p.lat_ny, nz = p.lat_nz;
+  const float h = (float)p.lat_h;
+  int x, yb, z;
+  const bool inb = tile_coords<2>(p, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, x, yb, z);
+  const float4 *P0 = p.fmapf, *P1 = p.fmapf + n, *P2 = p.fmapf + 2 * n;
+  int64_t ip[2];
+  bool vp[2];
+  float4 pa[2];
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    const int y = yb * 2 + q;
+    vp[q] = inb && y < ny;
+    ip[q] = vp[q] ? ((int64_t)x * ny + y) * nz + z : 0;
+    pa[q] = ldgf4(p.jit + ip[q]);
+  }
+  ForcePair pt;
+  pt.jx = make_float2(pa[0].x, pa[1].x), pt.jy = make_float2(pa[0].y, pa[1].y + h);
+  pt.jz = make_float2(pa[0].z, pa[1].z);
+  float2 fs[3], fc[3];
+  double corr[2][3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+    fs[c] = fc[c] = make_float2(0.0f, 0.0f), corr[0][c] = corr[1][c] = 0.0;
+  for (int g = 0; g < p.st.ngroups; ++g) {
+    const int4 gr = __ldg(p.st.groups + g);
+    const int cnt = gr.w >> 16, pos = gr.w & 0xffff, wd = pos >> 5, sh = pos & 31;
+    const uint32_t cm = cnt >= 32 ? ~0u : ((1u << cnt) - 1u);
+    uint32_t bits[2];
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      uint32_t m = vp[q] ? group_bits(__ldg(p.st.mask + (int64_t)wd * n + ip[q]), sh, cm) : 0u;
+      if (p.damage && m) {
+        const uint32_t bk = m & group_bits(p.st.broken[(int64_t)wd * n + ip[q]], sh, cm);
+        for (uint32_t f = bk; f; f &= f - 1) {  // broken bonds leave s_i
+          const int sl = pos + __ffs(f) - 1;
+          const float4 jj = p.jit[ip[q] + p.st.delta[sl]], o = p.st.e0[sl];
+          const float4 ji = p.jit[ip[q]];
+          corr[q][0] += (double)(jj.w * (o.x + (jj.x - ji.x)));
+          corr[q][1] += (double)(jj.w * (o.y + (jj.y - ji.y)));
+          corr[q][2] += (double)(jj.w * (o.z + (jj.z - ji.z)));
+        }
+        m &= ~bk;
+      }
+      bits[q] = m << q;
+    }
+    if (__all_sync(0xffffffffu, (bits[0] | bits[1]) == 0u))
+      continue;
+    const float gx = (float)gr.x * h, gz = (float)gr.y * h, by0 = (float)gr.z * h;
+    const int64_t jb = ((int64_t)(x + gr.x) * ny + (yb * 2 + gr.z)) * nz + (z + gr.y);
+    float2 part[3] = {make_float2(0.0f, 0.0f), make_float2(0.0f, 0.0f), make_float2(0.0f, 0.0f)};
+    if (UNROLL) {
+      static_assert(kUnrolledSlots == 12, "the cases below list the unrolled slot counts");
+      const int jb32 = (int)jb, nz32 = nz, n32 = (int)n;
+#define VPD_FORCE_CASE(C)                                                                 \
+  case C:                                                                                 \
+    force_pair_window<C, int>(p, cnt, jb32, nz32, n32, gx, gz, by0, h, pt, bits, part);   \
+    break;
+      switch (cnt) {
+        VPD_FORCE_CASE(1) VPD_FORCE_CASE(2) VPD_FORCE_CASE(3) VPD_FORCE_CASE(4)
+        VPD_FORCE_CASE(5) VPD_FORCE_CASE(6) VPD_FORCE_CASE(7) VPD_FORCE_CASE(8)
+        VPD_FORCE_CASE(9) VPD_FORCE_CASE(10) VPD_FORCE_CASE(11) VPD_FORCE_CASE(12)
+      default:
+        force_pair_window<0, int>(p, cnt, jb32, nz32, n32, gx, gz, by0, h, pt, bits, part);
+      }
+#undef VPD_FORCE_CASE
+    } else {
+      force_pair_window<0, int64_t>(p, cnt, jb, (int64_t)nz, n, gx, gz, by0, h, pt, bits, part);
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+      kahan_add2(fs[c], fc[c], part[c]);
+  }
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    if (!vp[q])
+      continue;
+    const int64_t i = ip[q];
+    const float4 a = P0[i], b = P1[i], c = P2[i], ji = p.jit[i];
+    const double4 s = p.vxi[i];
+    const double s0 = s.x - corr[q][0], s1 = s.y - corr[q][1], s2 = s.z - corr[q][2];
+    const double rv = 1.0 / (double)ji.w;
+    const float f0s = q ? fs[0].y : fs[0].x, f1s = q ? fs[1].y : fs[1].x, f2s = q ? fs[2].y : fs[2].x;
+    const double f0 = (double)f0s + (a.x * s0 + a.y * s1 + a.z * s2) * rv;
+    const double f1 = (double)f1s + (b.x * s0 + b.y * s1 + b.z * s2) * rv;
+    const double f2 = (double)f2s + (c.x * s0 + c.y * s1 + c.z * s2) * rv;
+    p.force[i] = make_double4(f0, f1, f2, 0.0);
+  }
+}
+
 // ------------------------------------------------------------------ launchers
 template <int kTileP> static unsigned tiled_grid(const StepParams &p) {
   const int64_t threads = (int64_t)p.lat_nx * ((p.lat_ny + kTileP - 1) / kTileP) * p.lat_nz;
@@ -370,38 +651,44 @@ template <int kTileP> static unsigned tiled_grid(const StepParams &p) {
 // 32-bit window indices need every index within a stencil reach of the lattice below 2^31
 static bool index32(const StepParams &p) { return p.n < (int64_t(1) << 30); }
 
-// With damage the deformation kernel keeps the runtime window loop: unrolled, the stretch
-// tests make it slower (0.28 against 0.25 ms on the 250k-point bar).
-template <int kTileP, bool UNROLL> static void launch_deformation(const StepParams &p, cudaStream_t s) {
-  if (p.damage)
-    k_deformation_tiled<true, kTileP, false><<<tiled_grid<kTileP>(p), kBondThreads, 0, s>>>(p);
-  else
-    k_deformation_tiled<false, kTileP, UNROLL><<<tiled_grid<kTileP>(p), kBondThreads, 0, s>>>(p);
+// With damage the deformation kernels keep the runtime window loop: unrolled, the stretch
+// tests made the scalar kernel slower (0.28 against 0.25 ms on the 250k-point bar).
+template <bool UNROLL> static void launch_deformation(const StepParams &p, cudaStream_t s) {
+  const unsigned grid = tiled_grid<2>(p);
+  if (p.tiled == 1) {
+    if (p.damage)
+      k_deformation_tiled<true, 2, false><<<grid, kBondThreads, 0, s>>>(p);
+    else
+      k_deformation_tiled<false, 2, UNROLL><<<grid, kBondThreads, 0, s>>>(p);
+  } else {
+    if (p.damage)
+      k_deformation_pair<true, false><<<grid, kBondThreads, 0, s>>>(p);
+    else
+      k_deformation_pair<false, UNROLL><<<grid, kBondThreads, 0, s>>>(p);
+  }
 }
 
-// points per thread: 2 unless VPD_BOND_KERNEL=tiled3 (read when the handle is created)
+// p.tiled: 1 the scalar two-point kernels, 2 the packed-pair ones (VPD_BOND_KERNEL, read when
+// the handle is created)
 int launch_deformation_tiled(const StepParams &p, cudaStream_t s) {
-  const bool u = index32(p);
-  if (p.tiled == 3)
-    u ? launch_deformation<3, true>(p, s) : launch_deformation<3, false>(p, s);
-  else
-    u ? launch_deformation<2, true>(p, s) : launch_deformation<2, false>(p, s);
+  index32(p) ? launch_deformation<true>(p, s) : launch_deformation<false>(p, s);
   VPD_CUDA(cudaGetLastError());
   return VPD_OK;
 }
 
 int launch_force_tiled(const StepParams &p, cudaStream_t s) {
   const bool u = index32(p);
-  if (p.tiled == 3) {
+  const unsigned grid = tiled_grid<2>(p);
+  if (p.tiled == 1) {
     if (u)
-      k_force_tiled<3, true><<<tiled_grid<3>(p), kBondThreads, 0, s>>>(p);
+      k_force_tiled<2, true><<<grid, kBondThreads, 0, s>>>(p);
     else
-      k_force_tiled<3, false><<<tiled_grid<3>(p), kBondThreads, 0, s>>>(p);
+      k_force_tiled<2, false><<<grid, kBondThreads, 0, s>>>(p);
   } else {
     if (u)
-      k_force_tiled<2, true><<<tiled_grid<2>(p), kBondThreads, 0, s>>>(p);
+      k_force_pair<true><<<grid, kBondThreads, 0, s>>>(p);
     else
-      k_force_tiled<2, false><<<tiled_grid<2>(p), kBondThreads, 0, s>>>(p);
+      k_force_pair<false><<<grid, kBondThreads, 0, s>>>(p);
   }
   VPD_CUDA(cudaGetLastError());
   return VPD_OK;
