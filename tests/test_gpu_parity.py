@@ -8,7 +8,7 @@ from conftest import golden, load_golden_timeseries, max_rel, nrmse
 
 import oracle as O
 import vpd
-from vpd.case import REFERENCE_JC_PROPS, Case, pd_coarse, tensile_bar
+from vpd.case import PRECISION_FP64, REFERENCE_JC_PROPS, Case, pd_coarse, tensile_bar
 
 pytestmark = pytest.mark.gpu
 torch = pytest.importorskip("torch")
@@ -209,6 +209,28 @@ def test_sliced_ell_layout_matches_stencil_layout(monkeypatch):
         assert nrmse(rb[:, STRESS], ra[:, STRESS]) < 1e-9
         assert max_rel(b.field("displacement"), ua) < 1e-9
         assert np.array_equal(b.field("damage_index"), da)
+
+
+@pytest.mark.parametrize("damage", [0, 1])
+def test_tiled_fp64_bond_kernels_match_slot_kernels_bitwise(monkeypatch, damage):
+    """The two-point tiled FP64 bond kernels sum every point's bonds in the per-slot kernels'
+    order with the same operations: on the jittered horizon-4 bar (ragged y extent, so one
+    column ends on a half tile) the increments agree bit for bit, bond breaking included."""
+    case = tensile_bar(3, nx=24, ny=21, nz=17, damage_mode=damage, damage_initiation=0.004,
+                       precision=PRECISION_FP64)
+    fields = ("displacement", "velocity", "stress_corotational", "state", "damage_index")
+    monkeypatch.setenv("VPD_BOND_KERNEL", "slot")
+    with vpd.Simulation(case) as a:
+        ra = a.step(150)
+        fa = {f: a.field(f) for f in fields}
+    monkeypatch.delenv("VPD_BOND_KERNEL")
+    with vpd.Simulation(case) as b:
+        rb = b.step(150)
+        for f in fields:
+            assert np.array_equal(b.field(f), fa[f]), f
+    assert np.array_equal(ra, rb)
+    if damage:
+        assert fa["damage_index"].max() > 0
 
 
 def test_graph_and_stage_launches_agree_bitwise():

@@ -422,8 +422,8 @@ int create_impl(vpd_handle *h, const vpd_case *c, const double *positions, const
   p.st = h->st;
   p.lat_nx = c->nx, p.lat_ny = c->ny, p.lat_nz = c->nz, p.lat_h = c->spacing;
   {
-    // VPD_BOND_KERNEL=slot selects the per-slot mixed-precision bond kernels, scalar the
-    // two-point tiled kernels in scalar FP32 (default: the packed-pair tiled kernels)
+    // VPD_BOND_KERNEL=slot selects the per-slot bond kernels (both precisions), scalar the
+    // two-point tiled mixed kernels in scalar FP32 (default: tiled, packed pairs when mixed)
     const char *bk = getenv("VPD_BOND_KERNEL");
     const std::string kind = bk ? bk : "";
     p.tiled = kind == "slot" ? 0 : (kind == "scalar" ? 1 : 2);

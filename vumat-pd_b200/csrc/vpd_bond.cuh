@@ -32,7 +32,32 @@ __device__ __forceinline__ void kahan_add2(float2 &s, float2 &c, float2 x) {  //
   s = t;
 }
 
-static __device__ __noinline__ bool exact_break_mixed(const double4 *xv, const double4 *U, int64_t i,
+// FP64 bond arithmetic shared by the per-slot (vpd_stencil.cu) and tiled (vpd_tiled64.cu)
+// kernels, every rounding spelled out so both produce the same bits.
+// G += (v d) (x) e for one bond (v: the neighbour's volume, or 0 without a bond).
+__device__ __forceinline__ void bond_deform64(double (&G)[9], double v, double d0, double d1, double d2, double e0,
+                                              double e1, double e2) {
+  const double w0 = __dmul_rn(v, d0), w1 = __dmul_rn(v, d1), w2 = __dmul_rn(v, d2);
+  G[0] = __fma_rn(w0, e0, G[0]), G[1] = __fma_rn(w0, e1, G[1]), G[2] = __fma_rn(w0, e2, G[2]);
+  G[3] = __fma_rn(w1, e0, G[3]), G[4] = __fma_rn(w1, e1, G[4]), G[5] = __fma_rn(w1, e2, G[5]);
+  G[6] = __fma_rn(w2, e0, G[6]), G[7] = __fma_rn(w2, e1, G[7]), G[8] = __fma_rn(w2, e2, G[8]);
+}
+// r . e, left to right
+__device__ __forceinline__ double dot3_rn(double r0, double r1, double r2, double e0, double e1, double e2) {
+  return __fma_rn(r2, e2, __fma_rn(r1, e1, __dmul_rn(r0, e0)));
+}
+// F = I + G K^-1 (row-major 3x3), each entry a left-to-right dot product
+__device__ __forceinline__ void deformation_from_g(const double (&G)[9], const double (&K)[9], double (&F)[9]) {
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = 0; b < 3; ++b)
+      F[3 * a + b] = __dadd_rn(a == b ? 1.0 : 0.0, dot3_rn(G[3 * a], G[3 * a + 1], G[3 * a + 2], K[b], K[3 + b], K[6 + b]));
+}
+
+// The exact FP64 critical-stretch decision of bond (i, j) (the reference's stretch formula,
+// every operation rounded as written).
+static __device__ __noinline__ bool exact_break(const double4 *xv, const double4 *U, int64_t i,
                                                int64_t j, double initiation, double failure,
                                                int use_compression) {
   const double4 xi = xv[i], xj = xv[j], ui = U[i], uj = U[j];
@@ -48,5 +73,64 @@ static __device__ __noinline__ bool exact_break_mixed(const double4 *xv, const d
   const double stretch = __ddiv_rn(__dsub_rn(cur, initial), initial);
   return stretch > initiation || (use_compression && stretch < -failure);
 }
+
+// ------------------------------------------------------------------ lattice tiling
+// Helpers of the tiled bond kernels (vpd_tiled.cu, vpd_tiled64.cu): a thread owns kTileP
+// points of one lattice column along y and walks the stencil's groups (runs of slots that
+// differ only in the y offset) as windows of consecutive lattice points.
+constexpr int kUnrolledSlots = 12;  // the switches below list counts 1 .. 12
+
+// Lattice coordinates of thread tau's column: z fastest, then the y-block, then x. Threads
+// past the lattice get the last column (their points are marked invalid).
+template <int kTileP>
+__device__ __forceinline__ bool tile_coords(const StepParams &p, int64_t tau, int &x, int &yb, int &z) {
+  const int nz = p.lat_nz, nyb = (p.lat_ny + kTileP - 1) / kTileP;
+  z = (int)(tau % nz);
+  const int64_t r = tau / nz;
+  yb = (int)(r % nyb);
+  x = (int)(r / nyb);
+  const bool inb = x < p.lat_nx;
+  x = inb ? x : p.lat_nx - 1;
+  return inb;
+}
+
+__device__ __forceinline__ uint32_t group_bits(uint32_t word, int shift, uint32_t cm) {
+  return (word >> shift) & cm;
+}
+
+template <typename I> __device__ __forceinline__ I clamp_to(I j, I n) { return j < 0 ? 0 : (j >= n ? n - 1 : j); }
+
+// Point i's bonds of one group (first slot pos, mask word wd, shift sh) that the stretch tests
+// flagged: `near` ones decided by the exact FP64 test, then both directed bonds of every
+// broken pair marked (bit k: slot pos + k).
+__device__ __forceinline__ void commit_breaks(const StepParams &p, int64_t i, int pos, int wd, int sh, uint32_t fr,
+                                              uint32_t nr) {
+  const int64_t n = p.n;
+  if (nr) {
+    const int64_t step = *p.step;
+    const double4 *U = (step & 1) ? p.u1 : p.u0;
+    for (uint32_t f = nr; f; f &= f - 1) {
+      const int k = __ffs(f) - 1;
+      if (exact_break(p.xv, U, i, i + p.st.delta[pos + k], p.dmg_initiation, p.dmg_failure, p.use_compression))
+        fr |= 1u << k;
+    }
+  }
+  if (fr) {
+    atomicOr(p.st.broken + (int64_t)wd * n + i, fr << sh);
+    for (uint32_t f = fr; f; f &= f - 1) {
+      const int sl = pos + __ffs(f) - 1;
+      const int r = p.st.reverse[sl];
+      atomicOr(p.st.broken + (int64_t)(r >> 5) * n + (i + p.st.delta[sl]), 1u << (r & 31));
+    }
+  }
+}
+
+template <int kTileP> static unsigned tiled_grid(const StepParams &p) {
+  const int64_t threads = (int64_t)p.lat_nx * ((p.lat_ny + kTileP - 1) / kTileP) * p.lat_nz;
+  return (unsigned)((threads + kBondThreads - 1) / kBondThreads);
+}
+
+// 32-bit window indices need every index within a stencil reach of the lattice below 2^31
+static inline bool index32(const StepParams &p) { return p.n < (int64_t(1) << 30); }
 
 }  // namespace vpd

@@ -75,7 +75,7 @@ __global__ void __launch_bounds__(kBondThreads, 3) k_deformation_mixed(StepParam
       const double4 *U = (step & 1) ? p.u1 : p.u0;
       for (uint32_t f = near; f; f &= f - 1) {
         const int b = __ffs(f) - 1;
-        if (exact_break_mixed(p.xv, U, i, i + dl[b], p.dmg_initiation, p.dmg_failure,
+        if (exact_break(p.xv, U, i, i + dl[b], p.dmg_initiation, p.dmg_failure,
                               p.use_compression))
           fresh |= 1u << b;
       }

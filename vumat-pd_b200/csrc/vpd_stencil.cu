@@ -18,17 +18,12 @@
 // Bond stretch is symmetric bit for bit ((i,j) and (j,i) see y and -y, xi and -xi), so the
 // critical-stretch test runs once per pair, by the point with the lower index ("forward"
 // slots, delta > 0), which sets the broken bit of both directed bonds.
-#include "vpd_math.cuh"
-#include "vpd_step.cuh"
+#include "vpd_bond.cuh"
 
 #include <algorithm>
 #include <vector>
 
 namespace vpd {
-
-__device__ __forceinline__ int64_t clamp_index(int64_t j, int64_t n) {
-  return j < 0 ? 0 : (j >= n ? n - 1 : j);
-}
 
 __device__ __forceinline__ void lattice_coords(int64_t i, int ny, int nz, int &x, int &y, int &z) {
   z = (int)(i % nz);
@@ -254,23 +249,6 @@ __global__ void __launch_bounds__(kBondThreads) k_shape_stencil(StepParams p) {
 }
 
 // ------------------------------------------------------------------ bond kernels
-__device__ __noinline__ bool exact_break_st(const double4 *xv, const double4 *U, int64_t i,
-                                            int64_t j, double initiation, double failure,
-                                            int use_compression) {
-  const double4 xi = xv[i], xj = xv[j], ui = U[i], uj = U[j];
-  const double yi0 = __dadd_rn(xi.x, ui.x), yi1 = __dadd_rn(xi.y, ui.y), yi2 = __dadd_rn(xi.z, ui.z);
-  const double y0 = __dsub_rn(__dadd_rn(xj.x, uj.x), yi0);
-  const double y1 = __dsub_rn(__dadd_rn(xj.y, uj.y), yi1);
-  const double y2 = __dsub_rn(__dadd_rn(xj.z, uj.z), yi2);
-  const double e0 = __dsub_rn(xj.x, xi.x), e1 = __dsub_rn(xj.y, xi.y), e2 = __dsub_rn(xj.z, xi.z);
-  const double initial =
-      __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(e0, e0), __dmul_rn(e1, e1)), __dmul_rn(e2, e2)));
-  const double cur =
-      __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(y0, y0), __dmul_rn(y1, y1)), __dmul_rn(y2, y2)));
-  const double stretch = __ddiv_rn(__dsub_rn(cur, initial), initial);
-  return stretch > initiation || (use_compression && stretch < -failure);
-}
-
 // F = I + [sum_j V_j (u_j - u_i) (x) xi] K^-1 over all bonds; with damage, the critical-stretch
 // test on each intact forward bond, breaking both directed bonds of a pair.
 template <bool DAMAGE>
@@ -301,10 +279,7 @@ __global__ void __launch_bounds__(kBondThreads, DAMAGE ? 2 : 3) k_deformation_st
       const double v = ((m >> b) & 1u) ? xj.w : 0.0;
       const double e0 = xj.x - xi.x, e1 = xj.y - xi.y, e2 = xj.z - xi.z;
       const double d0 = uj.x - ui.x, d1 = uj.y - ui.y, d2 = uj.z - ui.z;
-      const double w0 = v * d0, w1 = v * d1, w2 = v * d2;
-      G[0] += w0 * e0, G[1] += w0 * e1, G[2] += w0 * e2;
-      G[3] += w1 * e0, G[4] += w1 * e1, G[5] += w1 * e2;
-      G[6] += w2 * e0, G[7] += w2 * e1, G[8] += w2 * e2;
+      bond_deform64(G, v, d0, d1, d2, e0, e1, e2);
       if (DAMAGE && ((live >> b) & 1u)) {
         const double y0 = e0 + d0, y1 = e1 + d1, y2 = e2 + d2;
         const double yy = y0 * y0 + y1 * y1 + y2 * y2;
@@ -314,13 +289,13 @@ __global__ void __launch_bounds__(kBondThreads, DAMAGE ? 2 : 3) k_deformation_st
         if (yy > t * hi)
           broke = true;
         else if (yy >= t * lo)
-          broke = exact_break_st(p.xv, U, ii, j, p.dmg_initiation, p.dmg_failure, p.use_compression);
+          broke = exact_break(p.xv, U, ii, j, p.dmg_initiation, p.dmg_failure, p.use_compression);
         else if (p.use_compression) {
           const double c = p.compression2 * xx;
           if (yy < c * lo)
             broke = true;
           else if (yy <= c * hi)
-            broke = exact_break_st(p.xv, U, ii, j, p.dmg_initiation, p.dmg_failure, 1);
+            broke = exact_break(p.xv, U, ii, j, p.dmg_initiation, p.dmg_failure, 1);
         }
         if (broke)
           fresh |= 1u << b;
@@ -337,14 +312,14 @@ __global__ void __launch_bounds__(kBondThreads, DAMAGE ? 2 : 3) k_deformation_st
   }
   if (!valid)
     return;
-  double K[9], GK[9];
+  double K[9], F[9];
 #pragma unroll
   for (int c = 0; c < 9; ++c)
     K[c] = p.kinv[c * n + i];
-  m_mul(G, K, GK);
+  deformation_from_g(G, K, F);
 #pragma unroll
   for (int c = 0; c < 9; ++c)
-    p.F[c * n + i] = ((c % 4 == 0) ? 1.0 : 0.0) + GK[c];
+    p.F[c * n + i] = F[c];
 }
 
 // Bond sum of the force density over intact bonds,
@@ -380,9 +355,9 @@ __global__ void __launch_bounds__(kBondThreads, 3) k_force_stencil(StepParams p)
       const double4 a = ldg256(P0 + j), c = ldg256(P1 + j), d = ldg256(P2 + j);
       const double e0 = bond ? a.w - xi.x : 0.0, e1 = bond ? c.w - xi.y : 0.0,
                    e2 = bond ? d.w - xi.z : 0.0;
-      f0 += a.x * e0 + a.y * e1 + a.z * e2;
-      f1 += c.x * e0 + c.y * e1 + c.z * e2;
-      f2 += d.x * e0 + d.y * e1 + d.z * e2;
+      f0 = __dadd_rn(f0, dot3_rn(a.x, a.y, a.z, e0, e1, e2));
+      f1 = __dadd_rn(f1, dot3_rn(c.x, c.y, c.z, e0, e1, e2));
+      f2 = __dadd_rn(f2, dot3_rn(d.x, d.y, d.z, e0, e1, e2));
     }
   }
   if (!valid)
@@ -390,9 +365,9 @@ __global__ void __launch_bounds__(kBondThreads, 3) k_force_stencil(StepParams p)
   const double4 a = P0[i], c = P1[i], d = P2[i], s = p.vxi[i];
   const double s0 = s.x - c0, s1 = s.y - c1, s2 = s.z - c2;
   const double rv = 1.0 / xi.w;  // M_i = (V_i M_i) / V_i
-  f0 += (a.x * s0 + a.y * s1 + a.z * s2) * rv;
-  f1 += (c.x * s0 + c.y * s1 + c.z * s2) * rv;
-  f2 += (d.x * s0 + d.y * s1 + d.z * s2) * rv;
+  f0 = __dadd_rn(f0, __dmul_rn(dot3_rn(a.x, a.y, a.z, s0, s1, s2), rv));
+  f1 = __dadd_rn(f1, __dmul_rn(dot3_rn(c.x, c.y, c.z, s0, s1, s2), rv));
+  f2 = __dadd_rn(f2, __dmul_rn(dot3_rn(d.x, d.y, d.z, s0, s1, s2), rv));
   p.force[i] = make_double4(f0, f1, f2, 0.0);
 }
 

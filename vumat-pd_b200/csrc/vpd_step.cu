@@ -494,7 +494,7 @@ int launch_stage(int stage, const StepParams &p, cudaStream_t s) {
     if (p.mixed)
       return p.tiled ? launch_deformation_tiled(p, s) : launch_deformation_mixed(p, s);
     if (p.st.nw)
-      return launch_deformation_stencil(p, s);
+      return p.tiled ? launch_deformation_tiled64(p, s) : launch_deformation_stencil(p, s);
     k_deformation<<<bond_grid(p.n), kBondThreads, 0, s>>>(p);
   } else if (stage == 1) {
     if (p.surrogate)
@@ -504,7 +504,7 @@ int launch_stage(int stage, const StepParams &p, cudaStream_t s) {
     if (p.mixed)
       return p.tiled ? launch_force_tiled(p, s) : launch_force_mixed(p, s);
     if (p.st.nw)
-      return launch_force_stencil(p, s);
+      return p.tiled ? launch_force_tiled64(p, s) : launch_force_stencil(p, s);
     k_force<<<bond_grid(p.n), kBondThreads, 0, s>>>(p);
   } else {
     k_integrate<<<(unsigned)integrate_grid(p.n), kBondThreads, 0, s>>>(p);

@@ -50,7 +50,7 @@ struct StepParams {
   StencilLayout st;           // lattice-stencil layout; used instead of the ELL when st.nw > 0
   int lat_nx, lat_ny, lat_nz; // the lattice (points in index order (x ny + y) nz + z)
   double lat_h;               // lattice spacing
-  int tiled;                  // mixed precision bond kernels: 0 per slot, 1 tiled scalar, 2 tiled packed pairs
+  int tiled;                  // bond kernels: 0 per slot; mixed 1 tiled scalar, 2 tiled packed pairs; FP64 tiled
                               // (2 or 3), 0 for the per-slot kernels
   // kinematic state
   double4 *u0, *u1;           // displacement ping-pong: increment s reads u[s & 1]
@@ -125,5 +125,8 @@ int launch_mixed_setup(const StepParams &p, int ny, int nz, double h, double yof
 // tiled mixed-precision bond kernels (vpd_tiled.cu)
 int launch_deformation_tiled(const StepParams &p, cudaStream_t s);
 int launch_force_tiled(const StepParams &p, cudaStream_t s);
+// tiled FP64 bond kernels (vpd_tiled64.cu)
+int launch_deformation_tiled64(const StepParams &p, cudaStream_t s);
+int launch_force_tiled64(const StepParams &p, cudaStream_t s);
 
 }  // namespace vpd

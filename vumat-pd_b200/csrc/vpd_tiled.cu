@@ -23,28 +23,6 @@
 
 namespace vpd {
 
-constexpr int kUnrolledSlots = 12;  // the switches below list counts 1 .. 12
-
-// Lattice coordinates of thread tau's column: z fastest, then the y-block, then x. Threads
-// past the lattice get the last column (their points are marked invalid).
-template <int kTileP>
-__device__ __forceinline__ bool tile_coords(const StepParams &p, int64_t tau, int &x, int &yb, int &z) {
-  const int nz = p.lat_nz, nyb = (p.lat_ny + kTileP - 1) / kTileP;
-  z = (int)(tau % nz);
-  const int64_t r = tau / nz;
-  yb = (int)(r % nyb);
-  x = (int)(r / nyb);
-  const bool inb = x < p.lat_nx;
-  x = inb ? x : p.lat_nx - 1;
-  return inb;
-}
-
-__device__ __forceinline__ uint32_t group_bits(uint32_t word, int shift, uint32_t cm) {
-  return (word >> shift) & cm;
-}
-
-template <typename I> __device__ __forceinline__ I clamp_to(I j, I n) { return j < 0 ? 0 : (j >= n ? n - 1 : j); }
-
 // FP32 critical-stretch test of one live bond (reference xi = e, displacement difference d):
 // bit t of `fresh` when the bond is clearly broken, of `near` when it is within the 1e-5 margin
 // of a threshold and the exact FP64 test decides.
@@ -65,32 +43,6 @@ __device__ __forceinline__ void stretch_test(const StepParams &p, int t, float e
       fresh |= 1u << t;
     else if (yy <= c * hi)
       near |= 1u << t;
-  }
-}
-
-// Point i's bonds of one group (first slot pos, mask word wd, shift sh) that the stretch tests
-// flagged: `near` ones decided by the exact FP64 test, then both directed bonds of every
-// broken pair marked (bit k: slot pos + k).
-__device__ __forceinline__ void commit_breaks(const StepParams &p, int64_t i, int pos, int wd, int sh, uint32_t fr,
-                                              uint32_t nr) {
-  const int64_t n = p.n;
-  if (nr) {
-    const int64_t step = *p.step;
-    const double4 *U = (step & 1) ? p.u1 : p.u0;
-    for (uint32_t f = nr; f; f &= f - 1) {
-      const int k = __ffs(f) - 1;
-      if (exact_break_mixed(p.xv, U, i, i + p.st.delta[pos + k], p.dmg_initiation, p.dmg_failure,
-                            p.use_compression))
-        fr |= 1u << k;
-    }
-  }
-  if (fr) {
-    atomicOr(p.st.broken + (int64_t)wd * n + i, fr << sh);
-    for (uint32_t f = fr; f; f &= f - 1) {
-      const int sl = pos + __ffs(f) - 1;
-      const int r = p.st.reverse[sl];
-      atomicOr(p.st.broken + (int64_t)(r >> 5) * n + (i + p.st.delta[sl]), 1u << (r & 31));
-    }
   }
 }
 
@@ -643,14 +595,6 @@ __global__ void __launch_bounds__(kBondThreads, 2) k_force_pair(const __grid_con
 }
 
 // ------------------------------------------------------------------ launchers
-template <int kTileP> static unsigned tiled_grid(const StepParams &p) {
-  const int64_t threads = (int64_t)p.lat_nx * ((p.lat_ny + kTileP - 1) / kTileP) * p.lat_nz;
-  return (unsigned)((threads + kBondThreads - 1) / kBondThreads);
-}
-
-// 32-bit window indices need every index within a stencil reach of the lattice below 2^31
-static bool index32(const StepParams &p) { return p.n < (int64_t(1) << 30); }
-
 // With damage the deformation kernels keep the runtime window loop: unrolled, the stretch
 // tests made the scalar kernel slower (0.28 against 0.25 ms on the 250k-point bar).
 template <bool UNROLL> static void launch_deformation(const StepParams &p, cudaStream_t s) {
