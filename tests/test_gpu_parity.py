@@ -211,11 +211,13 @@ def test_sliced_ell_layout_matches_stencil_layout(monkeypatch):
         assert np.array_equal(b.field("damage_index"), da)
 
 
+@pytest.mark.parametrize("kind", ["", "tiled2"])
 @pytest.mark.parametrize("damage", [0, 1])
-def test_tiled_fp64_bond_kernels_match_slot_kernels_bitwise(monkeypatch, damage):
-    """The two-point tiled FP64 bond kernels sum every point's bonds in the per-slot kernels'
-    order with the same operations: on the jittered horizon-4 bar (ragged y extent, so one
-    column ends on a half tile) the increments agree bit for bit, bond breaking included."""
+def test_tiled_fp64_bond_kernels_match_slot_kernels_bitwise(monkeypatch, damage, kind):
+    """The tiled FP64 bond kernels (two points per thread along y; four in the force kernel
+    unless tiled2) sum every point's bonds in the per-slot kernels' order with the same
+    operations: on the jittered horizon-4 bar (y extent 21, so the last tile of a column is
+    ragged) the increments agree bit for bit, bond breaking included."""
     case = tensile_bar(3, nx=24, ny=21, nz=17, damage_mode=damage, damage_initiation=0.004,
                        precision=PRECISION_FP64)
     fields = ("displacement", "velocity", "stress_corotational", "state", "damage_index")
@@ -223,7 +225,7 @@ def test_tiled_fp64_bond_kernels_match_slot_kernels_bitwise(monkeypatch, damage)
     with vpd.Simulation(case) as a:
         ra = a.step(150)
         fa = {f: a.field(f) for f in fields}
-    monkeypatch.delenv("VPD_BOND_KERNEL")
+    monkeypatch.setenv("VPD_BOND_KERNEL", kind)
     with vpd.Simulation(case) as b:
         rb = b.step(150)
         for f in fields:

@@ -423,10 +423,11 @@ int create_impl(vpd_handle *h, const vpd_case *c, const double *positions, const
   p.lat_nx = c->nx, p.lat_ny = c->ny, p.lat_nz = c->nz, p.lat_h = c->spacing;
   {
     // VPD_BOND_KERNEL=slot selects the per-slot bond kernels (both precisions), scalar the
-    // two-point tiled mixed kernels in scalar FP32 (default: tiled, packed pairs when mixed)
+    // two-point tiled mixed kernels in scalar FP32, tiled2 the two-point FP64 force kernel
+    // (default: tiled, packed pairs when mixed, four points per thread in the FP64 force)
     const char *bk = getenv("VPD_BOND_KERNEL");
     const std::string kind = bk ? bk : "";
-    p.tiled = kind == "slot" ? 0 : (kind == "scalar" ? 1 : 2);
+    p.tiled = kind == "slot" ? 0 : (kind == "scalar" ? 1 : (kind == "tiled2" ? 3 : 2));
   }
   if (p.st.nw && ((rc = dalloc(h, &p.vxi, n)) ||
                   (c->precision != VPD_PRECISION_MIXED && (rc = dalloc(h, &p.fmap, 3 * n)))))

@@ -50,7 +50,7 @@ struct StepParams {
   StencilLayout st;           // lattice-stencil layout; used instead of the ELL when st.nw > 0
   int lat_nx, lat_ny, lat_nz; // the lattice (points in index order (x ny + y) nz + z)
   double lat_h;               // lattice spacing
-  int tiled;                  // bond kernels: 0 per slot; mixed 1 tiled scalar, 2 tiled packed pairs; FP64 tiled
+  int tiled;                  // bond kernels: 0 per slot; mixed 1 tiled scalar, else packed pairs; FP64 tiled (3: 2-point force)
                               // (2 or 3), 0 for the per-slot kernels
   // kinematic state
   double4 *u0, *u1;           // displacement ping-pong: increment s reads u[s & 1]

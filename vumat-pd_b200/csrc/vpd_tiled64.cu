@@ -161,14 +161,14 @@ __global__ void __launch_bounds__(kBondThreads, 2) k_deformation_tiled64(const _
 }
 
 // ------------------------------------------------------------------ force
-template <typename I>
-__device__ __forceinline__ void force64_element(const StepParams &p, int t, int cnt, I j, const double (&px)[2],
-                                                const double (&py)[2], const double (&pz)[2],
-                                                const uint32_t (&bits)[2], double (&f)[2][3]) {
+template <int P, typename I>
+__device__ __forceinline__ void force64_element(const StepParams &p, int t, int cnt, I j, const double (&px)[P],
+                                                const double (&py)[P], const double (&pz)[P],
+                                                const uint32_t (&bits)[P], double (&f)[P][3]) {
   const double4 *P0 = p.fmap, *P1 = p.fmap + p.n, *P2 = p.fmap + 2 * p.n;
   const double4 a = ldg256(P0 + j), c = ldg256(P1 + j), d = ldg256(P2 + j);
 #pragma unroll
-  for (int q = 0; q < 2; ++q) {
+  for (int q = 0; q < P; ++q) {
     if (t < q || t - q >= cnt)
       continue;
     const bool bond = (bits[q] >> t) & 1u;
@@ -179,90 +179,98 @@ __device__ __forceinline__ void force64_element(const StepParams &p, int t, int 
   }
 }
 
-template <int CNT, typename I>
-__device__ __forceinline__ void force64_window(const StepParams &p, int cnt, I jb, I nz, I n, const double (&px)[2],
-                                               const double (&py)[2], const double (&pz)[2],
-                                               const uint32_t (&bits)[2], double (&f)[2][3]) {
+template <int CNT, int P, typename I>
+__device__ __forceinline__ void force64_window(const StepParams &p, int cnt, I jb, I nz, I n, const double (&px)[P],
+                                               const double (&py)[P], const double (&pz)[P],
+                                               const uint32_t (&bits)[P], double (&f)[P][3]) {
   if constexpr (CNT > 0) {
 #pragma unroll
-    for (int t = 0; t < CNT + 1; ++t)
-      force64_element<I>(p, t, CNT, clamp_to<I>(jb + (I)t * nz, n), px, py, pz, bits, f);
+    for (int t = 0; t < CNT + P - 1; ++t)
+      force64_element<P, I>(p, t, CNT, clamp_to<I>(jb + (I)t * nz, n), px, py, pz, bits, f);
   } else {
-    for (int t = 0; t < cnt + 1; ++t)
-      force64_element<I>(p, t, cnt, clamp_to<I>(jb + (I)t * nz, n), px, py, pz, bits, f);
+    for (int t = 0; t < cnt + P - 1; ++t)
+      force64_element<P, I>(p, t, cnt, clamp_to<I>(jb + (I)t * nz, n), px, py, pz, bits, f);
   }
 }
 
 // f_i = sum_j V_j M_j xi over intact bonds + M_i s_i, s_i = vxi_i - sum_{broken j} V_j xi: a
 // bond reads the three force-map records of j (its coordinates ride in their fourth lane).
-template <bool UNROLL>
+// kTileP points per thread along y.
+template <int kTileP, bool UNROLL>
 __global__ void __launch_bounds__(kBondThreads, 2) k_force_tiled64(const __grid_constant__ StepParams p) {
+  constexpr int P = kTileP;
   const int64_t n = p.n;
   const int ny = p.lat_ny, nz = p.lat_nz;
   int x, yb, z;
-  const bool inb = tile_coords<2>(p, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, x, yb, z);
-  int64_t ip[2];
-  bool vp[2];
-  double px[2], py[2], pz[2], rv[2];
+  const bool inb = tile_coords<P>(p, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, x, yb, z);
+  int64_t ip[P];
+  bool vp[P];
+  double px[P], py[P], pz[P], f[P][3];
 #pragma unroll
-  for (int q = 0; q < 2; ++q) {
-    const int y = yb * 2 + q;
+  for (int q = 0; q < P; ++q) {
+    const int y = yb * P + q;
     vp[q] = inb && y < ny;
     ip[q] = vp[q] ? ((int64_t)x * ny + y) * nz + z : 0;
     const double4 xi = ldg256(p.xv + ip[q]);
-    px[q] = xi.x, py[q] = xi.y, pz[q] = xi.z, rv[q] = xi.w;
+    px[q] = xi.x, py[q] = xi.y, pz[q] = xi.z;
+    f[q][0] = f[q][1] = f[q][2] = 0.0;
   }
-  double f[2][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}}, corr[2][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
+  bool any_broken = false;  // corrections for broken bonds are rare: gathered after the sum
   for (int g = 0; g < p.st.ngroups; ++g) {
     const int4 gr = __ldg(p.st.groups + g);
     const int cnt = gr.w >> 16, pos = gr.w & 0xffff, wd = pos >> 5, sh = pos & 31;
     const uint32_t cm = cnt >= 32 ? ~0u : ((1u << cnt) - 1u);
-    uint32_t bits[2];
+    uint32_t bits[P], any = 0u;
 #pragma unroll
-    for (int q = 0; q < 2; ++q) {
+    for (int q = 0; q < P; ++q) {
       uint32_t m = vp[q] ? group_bits(__ldg(p.st.mask + (int64_t)wd * n + ip[q]), sh, cm) : 0u;
       if (p.damage && m) {
         const uint32_t bk = m & group_bits(p.st.broken[(int64_t)wd * n + ip[q]], sh, cm);
-        for (uint32_t b = bk; b; b &= b - 1) {  // broken bonds leave s_i
-          const double4 xj = p.xv[ip[q] + p.st.delta[pos + __ffs(b) - 1]];
-          corr[q][0] += xj.w * (xj.x - px[q]), corr[q][1] += xj.w * (xj.y - py[q]);
-          corr[q][2] += xj.w * (xj.z - pz[q]);
-        }
+        any_broken |= bk != 0u;
         m &= ~bk;
       }
-      bits[q] = m << q;
+      bits[q] = m << q;  // bit t: the neighbour at window position t (slot pos + t - q)
+      any |= bits[q];
     }
-    if (__all_sync(0xffffffffu, (bits[0] | bits[1]) == 0u))
+    if (__all_sync(0xffffffffu, any == 0u))
       continue;
-    const int64_t jb = ((int64_t)(x + gr.x) * ny + (yb * 2 + gr.z)) * nz + (z + gr.y);
+    const int64_t jb = ((int64_t)(x + gr.x) * ny + (yb * P + gr.z)) * nz + (z + gr.y);
     if (UNROLL) {
       static_assert(kUnrolledSlots == 12, "the cases below list the unrolled slot counts");
       const int jb32 = (int)jb, nz32 = nz, n32 = (int)n;
 #define VPD_FORCE64_CASE(C)                                                       \
   case C:                                                                         \
-    force64_window<C, int>(p, cnt, jb32, nz32, n32, px, py, pz, bits, f);         \
+    force64_window<C, P, int>(p, cnt, jb32, nz32, n32, px, py, pz, bits, f);      \
     break;
       switch (cnt) {
         VPD_FORCE64_CASE(1) VPD_FORCE64_CASE(2) VPD_FORCE64_CASE(3) VPD_FORCE64_CASE(4)
         VPD_FORCE64_CASE(5) VPD_FORCE64_CASE(6) VPD_FORCE64_CASE(7) VPD_FORCE64_CASE(8)
         VPD_FORCE64_CASE(9) VPD_FORCE64_CASE(10) VPD_FORCE64_CASE(11) VPD_FORCE64_CASE(12)
       default:
-        force64_window<0, int>(p, cnt, jb32, nz32, n32, px, py, pz, bits, f);
+        force64_window<0, P, int>(p, cnt, jb32, nz32, n32, px, py, pz, bits, f);
       }
 #undef VPD_FORCE64_CASE
     } else {
-      force64_window<0, int64_t>(p, cnt, jb, (int64_t)nz, n, px, py, pz, bits, f);
+      force64_window<0, P, int64_t>(p, cnt, jb, (int64_t)nz, n, px, py, pz, bits, f);
     }
   }
   const double4 *P0 = p.fmap, *P1 = p.fmap + n, *P2 = p.fmap + 2 * n;
 #pragma unroll
-  for (int q = 0; q < 2; ++q) {
+  for (int q = 0; q < P; ++q) {
     if (!vp[q])
       continue;
     const int64_t i = ip[q];
+    // s_i less the broken bonds' V_j xi, summed in slot order
+    double c0 = 0.0, c1 = 0.0, c2 = 0.0;
+    if (any_broken)
+      for (int w = 0; w < p.st.nw; ++w)
+        for (uint32_t b = p.st.mask[(int64_t)w * n + i] & p.st.broken[(int64_t)w * n + i]; b; b &= b - 1) {
+          const double4 xj = p.xv[i + p.st.delta[32 * w + __ffs(b) - 1]];
+          c0 += xj.w * (xj.x - px[q]), c1 += xj.w * (xj.y - py[q]), c2 += xj.w * (xj.z - pz[q]);
+        }
     const double4 a = P0[i], c = P1[i], d = P2[i], s = p.vxi[i];
-    const double s0 = s.x - corr[q][0], s1 = s.y - corr[q][1], s2 = s.z - corr[q][2];
-    const double r = 1.0 / rv[q];  // M_i = (V_i M_i) / V_i
+    const double s0 = s.x - c0, s1 = s.y - c1, s2 = s.z - c2;
+    const double r = 1.0 / p.xv[i].w;  // M_i = (V_i M_i) / V_i
     const double f0 = __dadd_rn(f[q][0], __dmul_rn(dot3_rn(a.x, a.y, a.z, s0, s1, s2), r));
     const double f1 = __dadd_rn(f[q][1], __dmul_rn(dot3_rn(c.x, c.y, c.z, s0, s1, s2), r));
     const double f2 = __dadd_rn(f[q][2], __dmul_rn(dot3_rn(d.x, d.y, d.z, s0, s1, s2), r));
@@ -285,12 +293,21 @@ int launch_deformation_tiled64(const StepParams &p, cudaStream_t s) {
   return VPD_OK;
 }
 
+// four points per thread (two with VPD_BOND_KERNEL=tiled2)
 int launch_force_tiled64(const StepParams &p, cudaStream_t s) {
-  const unsigned grid = tiled_grid<2>(p);
-  if (index32(p))
-    k_force_tiled64<true><<<grid, kBondThreads, 0, s>>>(p);
-  else
-    k_force_tiled64<false><<<grid, kBondThreads, 0, s>>>(p);
+  if (p.tiled == 3) {
+    const unsigned grid = tiled_grid<2>(p);
+    if (index32(p))
+      k_force_tiled64<2, true><<<grid, kBondThreads, 0, s>>>(p);
+    else
+      k_force_tiled64<2, false><<<grid, kBondThreads, 0, s>>>(p);
+  } else {
+    const unsigned grid = tiled_grid<4>(p);
+    if (index32(p))
+      k_force_tiled64<4, true><<<grid, kBondThreads, 0, s>>>(p);
+    else
+      k_force_tiled64<4, false><<<grid, kBondThreads, 0, s>>>(p);
+  }
   VPD_CUDA(cudaGetLastError());
   return VPD_OK;
 }
