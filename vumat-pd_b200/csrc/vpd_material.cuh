@@ -34,24 +34,25 @@ __device__ __forceinline__ void block_partials(double (&v)[K], double *out, int6
   }
 }
 
-// One point's material context between the kinematics and the stress update.
+// One point's material context across the constitutive update. The kinematic history (F, V,
+// R, E) is written as soon as it is formed (material_load), so of the kinematics only F and R
+// (the force map's and the stress rotation's inputs) stay live across the return map.
 struct MaterialPoint {
-  double F[9];      // deformation gradient of this increment
-  Corotational co;  // rotation, left stretch, unrotated rate of deformation
-  double E[6], Eold[6], oldFull[9];
-  double inc[6];    // corotational strain increment (Voigt, tensor shear)
-  JcPoint pt;       // VUMAT stress, state and energies (old on entry to the update)
+  double F[9];    // deformation gradient of this increment
+  double R[9];    // rotation R_{n+1}
+  double inc[6];  // corotational strain increment (Voigt, tensor shear)
+  double dE[6];   // E_{n+1} - E_n, for the internal-energy diagnostic
+  double eAxis;   // E_{n+1} along the loading axis, for the observation-window mean
+  bool eFinite;   // every component of E_{n+1} finite
+  JcPoint pt;     // VUMAT stress, state and energies (old on entry to the update)
 };
 
 __device__ __forceinline__ void material_load(const StepParams &p, int64_t i, MaterialPoint &m) {
   const int64_t n = p.n;
-  double(&F)[9] = m.F;
-  Corotational &co = m.co;
-  double(&E)[6] = m.E;
-  double(&Eold)[6] = m.Eold;
-  double(&oldFull)[9] = m.oldFull;
   JcPoint &pt = m.pt;
-  double Fn[9], Vn[9], Rn[9];
+  double(&F)[9] = m.F;
+  double Fn[9], Vn[9], Rn[9], Eold[6];
+  // every load first (one memory round trip; the stores below would otherwise order them)
   if (p.mixed) {  // F = I + G K^-1 in FP64 from the FP32 bond sum
     double G[9], K[9];
 #pragma unroll
@@ -72,13 +73,6 @@ __device__ __forceinline__ void material_load(const StepParams &p, int64_t i, Ma
     Vn[c] = p.Vn[c * n + i];
     Rn[c] = p.Rn[c * n + i];
   }
-  if (!corotational_update(Fn, F, Vn, Rn, p.dt, co)) {
-    atomicOr(p.status, STATUS_SINGULAR_KINEMATICS);
-#pragma unroll
-    for (int c = 0; c < 9; ++c)
-      co.dbar[c] = 0.0, co.spin[c] = 0.0, co.r[c] = Rn[c], co.v[c] = Vn[c];
-  }
-  green_lagrange6(F, E);
 #pragma unroll
   for (int c = 0; c < 6; ++c) {
     Eold[c] = p.En[c * n + i];
@@ -87,7 +81,33 @@ __device__ __forceinline__ void material_load(const StepParams &p, int64_t i, Ma
   }
   pt.eInternal = p.eI[i];
   pt.eInelastic = p.eP[i];
-  voigt_to_full(pt.stress, oldFull);
+  Corotational co;
+  if (!corotational_update(Fn, F, Vn, Rn, p.dt, co)) {
+    atomicOr(p.status, STATUS_SINGULAR_KINEMATICS);
+#pragma unroll
+    for (int c = 0; c < 9; ++c)
+      co.dbar[c] = 0.0, co.spin[c] = 0.0, co.r[c] = Rn[c], co.v[c] = Vn[c];
+  }
+  double E[6];
+  green_lagrange6(F, E);
+  // kinematic history of this increment, committed now
+#pragma unroll
+  for (int c = 0; c < 9; ++c) {
+    p.Fn[c * n + i] = F[c];
+    p.Vn[c * n + i] = co.v[c];
+    p.Rn[c * n + i] = co.r[c];
+    m.R[c] = co.r[c];
+  }
+  m.eFinite = true;
+#pragma unroll
+  for (int c = 0; c < 6; ++c) {
+    m.dE[c] = E[c] - Eold[c];
+    p.En[c * n + i] = E[c];
+    m.eFinite = m.eFinite && isfinite(E[c]);
+  }
+  // selects rather than a runtime index, which would put the array in local memory
+  const int ax = p.bc.axis;
+  m.eAxis = ax == 0 ? E[0] : (ax == 1 ? E[1] : E[2]);
   const double *d = co.dbar;
   m.inc[0] = d[0] * p.dt, m.inc[1] = d[4] * p.dt, m.inc[2] = d[8] * p.dt;
   m.inc[3] = 0.5 * (d[5] + d[7]) * p.dt, m.inc[4] = 0.5 * (d[2] + d[6]) * p.dt;
@@ -95,32 +115,27 @@ __device__ __forceinline__ void material_load(const StepParams &p, int64_t i, Ma
 }
 
 // part[PM_*] and maxEqps receive this point's diagnostic contributions.
-__device__ __forceinline__ void material_store(const StepParams &p, int64_t i, MaterialPoint &m, double *part,
+__device__ __forceinline__ void material_store(const StepParams &p, int64_t i, const MaterialPoint &m, double *part,
                                                double &maxEqps) {
   const int64_t n = p.n;
-  const double(&F)[9] = m.F;
-  const Corotational &co = m.co;
-  const double(&E)[6] = m.E;
-  const double(&Eold)[6] = m.Eold;
-  const double(&oldFull)[9] = m.oldFull;
   const JcPoint &pt = m.pt;
-  double full[9], spatial[9], K[9], M[9];
-  voigt_to_full(pt.stress, full);
-  rotate_to_spatial(full, co.r, spatial);
+  const double(&F)[9] = m.F;
+  const double(&R)[9] = m.R;
+  double K[9], old[6], oldFull[9], full[9], spatial[9], M[9];
 #pragma unroll
   for (int c = 0; c < 9; ++c)
     K[c] = p.kinv[c * n + i];
+#pragma unroll
+  for (int c = 0; c < 6; ++c)
+    old[c] = p.sig[c * n + i];  // the old stress, still in place
+  voigt_to_full(old, oldFull);
+  voigt_to_full(pt.stress, full);
+  rotate_to_spatial(full, R, spatial);
   if (!force_map(spatial, F, K, M)) {
     atomicOr(p.status, STATUS_SINGULAR_F);
 #pragma unroll
     for (int c = 0; c < 9; ++c)
       M[c] = 0.0;
-  }
-#pragma unroll
-  for (int c = 0; c < 9; ++c) {
-    p.Fn[c * n + i] = F[c];
-    p.Vn[c * n + i] = co.v[c];
-    p.Rn[c * n + i] = co.r[c];
   }
   // the force map scaled by the point's volume, in the layout the force kernel gathers
   const double4 xi = p.xv[i];
@@ -147,7 +162,6 @@ __device__ __forceinline__ void material_store(const StepParams &p, int64_t i, M
   }
 #pragma unroll
   for (int c = 0; c < 6; ++c) {
-    p.En[c * n + i] = E[c];
     p.sig[c * n + i] = pt.stress[c];
     p.state[c * n + i] = pt.state[c];
   }
@@ -158,26 +172,23 @@ __device__ __forceinline__ void material_store(const StepParams &p, int64_t i, M
   const double a0 = 0.5 * (oldFull[0] + spatial[0]), a4 = 0.5 * (oldFull[4] + spatial[4]);
   const double a8 = 0.5 * (oldFull[8] + spatial[8]), a1 = 0.5 * (oldFull[1] + spatial[1]);
   const double a2 = 0.5 * (oldFull[2] + spatial[2]), a5 = 0.5 * (oldFull[5] + spatial[5]);
-  const double e11 = E[0] - Eold[0], e22 = E[1] - Eold[1], e33 = E[2] - Eold[2];
-  const double e23 = E[3] - Eold[3], e13 = E[4] - Eold[4], e12 = E[5] - Eold[5];
-  part[PM_DU] = (a0 * e11 + a4 * e22 + a8 * e33 + 2.0 * (a1 * e12 + a2 * e13 + a5 * e23)) * vol;
+  const double *dE = m.dE;
+  part[PM_DU] = (a0 * dE[0] + a4 * dE[1] + a8 * dE[2] + 2.0 * (a1 * dE[5] + a2 * dE[4] + a5 * dE[3])) * vol;
   const double w = p.obsw[i];
   if (w > 0.0) {
-    // selects rather than a runtime index, which would put the arrays in local memory
     const int ax = p.bc.axis;
     const double sa = ax == 0 ? spatial[0] : (ax == 1 ? spatial[4] : spatial[8]);
-    const double ea = ax == 0 ? E[0] : (ax == 1 ? E[1] : E[2]);
     part[PM_AVG_STRESS] = p.sign * sa * w;
-    part[PM_AVG_STRAIN] = p.sign * ea * w;
+    part[PM_AVG_STRAIN] = p.sign * m.eAxis * w;
   }
   maxEqps = pt.state[1];
-  bool fin = true;
+  bool fin = m.eFinite;
 #pragma unroll
   for (int c = 0; c < 9; ++c)
     fin = fin && isfinite(spatial[c]);
 #pragma unroll
   for (int c = 0; c < 6; ++c)
-    fin = fin && isfinite(E[c]) && isfinite(pt.state[c]);
+    fin = fin && isfinite(pt.state[c]);
   part[PM_NONFINITE] = fin ? 0.0 : 1.0;
   part[PM_PLASTIC] = pt.state[4] > 0.0 ? 1.0 : 0.0;
 }

@@ -19,8 +19,9 @@
 namespace vpd {
 
 // ------------------------------------------------------------------ forward
-// smem: W1 (128x16) | W2 (128x128) | W3 | W4 (16x128) | A (128x128) | X0 (128x16) | barrier
-constexpr size_t kFwdSmem = 4096 + 32768 + 32768 + 4096 + 32768 + 4096 + 64;
+// smem: W1 (128x16) | W2 (128x128) | W3 | W4 (16x128) | A (128x128) | X0 (128x16) | barrier |
+//       biases
+constexpr size_t kFwdSmem = 4096 + 32768 + 32768 + 4096 + 32768 + 4096 + 64 + 4 * kBiasFloats;
 
 __device__ __forceinline__ void stage_weights_fwd(unsigned char *s, const MlpWeights &w) {
   stage_rowmajor(s, w.w1, kMlpHidden, kMlpIn);
@@ -35,6 +36,7 @@ __global__ void __launch_bounds__(128, 1) k_mlp_forward(MlpWeights w, const floa
   unsigned char *sW1 = smem, *sW2 = smem + 4096, *sW3 = sW2 + 32768, *sW4 = sW3 + 32768;
   unsigned char *sA = sW4 + 4096, *sX = sA + 32768;
   uint64_t *mbar = reinterpret_cast<uint64_t *>(sX + 4096);
+  float *sBias = reinterpret_cast<float *>(sX + 4096 + 64);
   __shared__ uint32_t s_tmem;
   const int t = threadIdx.x;
   const int64_t row = (int64_t)blockIdx.x * 128 + t;
@@ -43,6 +45,7 @@ __global__ void __launch_bounds__(128, 1) k_mlp_forward(MlpWeights w, const floa
   if (t == 0)
     umma::mbar_init(mbar, 1);
   stage_weights_fwd(smem, w);
+  stage_biases(sBias, w);
   float xin[kMlpIn];
 #pragma unroll
   for (int c = 0; c < kMlpIn; ++c)
@@ -54,6 +57,7 @@ __global__ void __launch_bounds__(128, 1) k_mlp_forward(MlpWeights w, const floa
 #pragma unroll
     for (int c = 0; c < kMlpIn; ++c)
       acts.y0[row * kMlpIn + c] = __float2bfloat16(xin[c]);
+  stage_wait();
   umma::fence_before_sync();
   __syncthreads();
   umma::fence_after_sync();
@@ -62,13 +66,13 @@ __global__ void __launch_bounds__(128, 1) k_mlp_forward(MlpWeights w, const floa
   Sync sy{mbar, 0u, err, 1u, true};
   const bool keep = row < B;
   gemm(sy, tmem, sX, sW1, kMlpIn, kMlpHidden);
-  hidden_epilogue(trow, w.b1, sA, keep && acts.z1 ? acts.z1 + row * kMlpHidden : nullptr,
+  hidden_epilogue(trow, sBias, sA, keep && acts.z1 ? acts.z1 + row * kMlpHidden : nullptr,
                   keep && acts.y1 ? acts.y1 + row * kMlpHidden : nullptr);
   gemm(sy, tmem, sA, sW2, kMlpHidden, kMlpHidden);
-  hidden_epilogue(trow, w.b2, sA, keep && acts.z2 ? acts.z2 + row * kMlpHidden : nullptr,
+  hidden_epilogue(trow, sBias + kMlpHidden, sA, keep && acts.z2 ? acts.z2 + row * kMlpHidden : nullptr,
                   keep && acts.y2 ? acts.y2 + row * kMlpHidden : nullptr);
   gemm(sy, tmem, sA, sW3, kMlpHidden, kMlpHidden);
-  hidden_epilogue(trow, w.b3, sA, keep && acts.z3 ? acts.z3 + row * kMlpHidden : nullptr,
+  hidden_epilogue(trow, sBias + 2 * kMlpHidden, sA, keep && acts.z3 ? acts.z3 + row * kMlpHidden : nullptr,
                   keep && acts.y3 ? acts.y3 + row * kMlpHidden : nullptr);
   gemm(sy, tmem, sA, sW4, kMlpHidden, kMlpOut);
   float v[16];
@@ -154,6 +158,7 @@ __global__ void __launch_bounds__(128, 1) k_mlp_backward(MlpWeights w, const __n
   stage_rowmajor(sWt2, wt, kMlpHidden, kMlpHidden);
   stage_rowmajor(sWt3, wt + 16384, kMlpHidden, kMlpHidden);
   stage_rowmajor(sWt4, wt + 32768, kMlpHidden, kMlpOut);
+  stage_wait();
   umma::fence_before_sync();
   __syncthreads();
   umma::fence_after_sync();

@@ -36,15 +36,19 @@ __device__ __forceinline__ void st_bf16(unsigned char *tile, int row, int k, int
   *reinterpret_cast<__nv_bfloat16 *>(tile + kmajor_offset(row, k, ktotal)) = __float2bfloat16(v);
 }
 
-// Copies a row-major bf16 matrix [rows][cols] into a K-major tile (K = cols), 16 bytes at a time.
+// Copies a row-major bf16 matrix [rows][cols] (16-byte aligned) into a K-major tile (K = cols),
+// 16 bytes at a time with cp.async: every copy of the thread is in flight at once. The copies
+// complete at stage_wait(), which every thread calls before the barrier that publishes them.
 __device__ __forceinline__ void stage_rowmajor(unsigned char *tile, const __nv_bfloat16 *src, int rows, int cols) {
   const int chunks = rows * cols / 8;
   for (int c = threadIdx.x; c < chunks; c += blockDim.x) {
     const int row = c / (cols / 8), k = (c % (cols / 8)) * 8;
-    *reinterpret_cast<uint4 *>(tile + kmajor_offset(row, k, cols)) =
-        *reinterpret_cast<const uint4 *>(src + (size_t)row * cols + k);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(tile + kmajor_offset(row, k, cols))),
+                 "l"(src + (size_t)row * cols + k)
+                 : "memory");
   }
 }
+__device__ __forceinline__ void stage_wait() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 struct Sync {
   uint64_t *mbar;
@@ -78,34 +82,48 @@ __device__ __forceinline__ void gemm(Sync &sy, uint32_t tmem_d, const unsigned c
   sy.wait();
 }
 
-// Hidden-layer epilogue for the calling thread's row: bias, SiLU, next operand (bf16) in A;
-// optionally the pre-activation and activation to global memory.
+// The network's biases (b1, b2, b3: 128 each; b4: 16) copied into shared memory once per block:
+// the epilogues read them as broadcast 16-byte loads.
+constexpr int kBiasFloats = 3 * kMlpHidden + kMlpOut;
+__device__ __forceinline__ void stage_biases(float *dst, const MlpWeights &w) {
+  for (int c = threadIdx.x; c < kBiasFloats; c += blockDim.x)
+    dst[c] = c < kMlpHidden ? w.b1[c]
+                            : (c < 2 * kMlpHidden ? w.b2[c - kMlpHidden]
+                                                  : (c < 3 * kMlpHidden ? w.b3[c - 2 * kMlpHidden]
+                                                                        : w.b4[c - 3 * kMlpHidden]));
+}
+
+// Hidden-layer epilogue for the calling thread's row, 32 columns per TMEM load: bias, SiLU,
+// next operand (bf16) in A; optionally the pre-activation and activation to global memory.
+// `bias` points at the layer's 128 biases (shared or global memory, 16-byte aligned).
 __device__ __forceinline__ void hidden_epilogue(uint32_t trow, const float *bias, unsigned char *A, float *z_out,
                                                 __nv_bfloat16 *y_out) {
   const int t = threadIdx.x;
-  for (int c0 = 0; c0 < kMlpHidden; c0 += 16) {
-    float v[16];
-    umma::tmem_ld16(trow + c0, v);
-    __align__(16) float bb[16];
+#pragma unroll 1
+  for (int c0 = 0; c0 < kMlpHidden; c0 += 32) {
+    float v[32];
+    umma::tmem_ld32(trow + c0, v);
+    __align__(16) __nv_bfloat16 yb[32];
 #pragma unroll
-    for (int q = 0; q < 4; ++q)  // the bias row, four 16-byte loads (same for every thread)
-      *reinterpret_cast<float4 *>(bb + 4 * q) = __ldg(reinterpret_cast<const float4 *>(bias + c0) + q);
-    __align__(16) __nv_bfloat16 yb[16];
+    for (int q = 0; q < 8; ++q) {
+      const float4 bb = *reinterpret_cast<const float4 *>(bias + c0 + 4 * q);
+      const float z[4] = {v[4 * q] + bb.x, v[4 * q + 1] + bb.y, v[4 * q + 2] + bb.z, v[4 * q + 3] + bb.w};
 #pragma unroll
-    for (int c = 0; c < 16; ++c) {
-      const float z = v[c] + bb[c];
-      yb[c] = __float2bfloat16(silu(z));
-      if (z_out)
-        z_out[c0 + c] = z;
+      for (int c = 0; c < 4; ++c) {
+        yb[4 * q + c] = __float2bfloat16(silu(z[c]));
+        if (z_out)
+          z_out[c0 + 4 * q + c] = z[c];
+      }
     }
-    // two 16-byte rows of core matrices
-    *reinterpret_cast<uint4 *>(A + kmajor_offset(t, c0, kMlpHidden)) = *reinterpret_cast<const uint4 *>(yb);
-    *reinterpret_cast<uint4 *>(A + kmajor_offset(t, c0 + 8, kMlpHidden)) =
-        *reinterpret_cast<const uint4 *>(yb + 8);
-    if (y_out) {
-      *reinterpret_cast<uint4 *>(y_out + c0) = *reinterpret_cast<const uint4 *>(yb);
-      *reinterpret_cast<uint4 *>(y_out + c0 + 8) = *reinterpret_cast<const uint4 *>(yb + 8);
-    }
+    // four 16-byte rows of core matrices
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      *reinterpret_cast<uint4 *>(A + kmajor_offset(t, c0 + 8 * k, kMlpHidden)) =
+          *reinterpret_cast<const uint4 *>(yb + 8 * k);
+    if (y_out)
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        *reinterpret_cast<uint4 *>(y_out + c0 + 8 * k) = *reinterpret_cast<const uint4 *>(yb + 8 * k);
   }
 }
 

@@ -394,11 +394,11 @@ int train_surrogate(const vpd_surrogate_config &cfg, uint16_t *w_out, float *b_o
 
 // ------------------------------------------------------------------ fused material kernel
 // smem: W1 | W2 | W3 | W4 | A (128 x 128; the layer-1 input X sits in its first 4 KB, dead
-// once the first product has completed) | mbarrier
-constexpr size_t kSurrSmem = 4096 + 32768 + 32768 + 4096 + 32768 + 64;
+// once the first product has completed) | mbarrier | biases
+constexpr size_t kSurrSmem = 4096 + 32768 + 32768 + 4096 + 32768 + 64 + 4 * kBiasFloats;
 
 template <bool NET>
-__global__ void __launch_bounds__(kMaterialThreads, 2) k_material_surrogate(const __grid_constant__ StepParams p) {
+__global__ void __launch_bounds__(kMaterialThreads, NET ? 2 : 4) k_material_surrogate(const __grid_constant__ StepParams p) {
   extern __shared__ __align__(1024) unsigned char smem[];
   __shared__ uint32_t s_tmem;
   const int t = threadIdx.x;
@@ -406,6 +406,7 @@ __global__ void __launch_bounds__(kMaterialThreads, 2) k_material_surrogate(cons
   unsigned char *sW1 = smem, *sW2 = smem + 4096, *sW3 = sW2 + 32768, *sW4 = sW3 + 32768, *sA = sW4 + 4096;
   unsigned char *sX = sA;
   uint64_t *mbar = reinterpret_cast<uint64_t *>(sA + 32768);
+  float *sBias = reinterpret_cast<float *>(sA + 32768 + 64);
   const MlpWeights w = mlp_weights(reinterpret_cast<const __nv_bfloat16 *>(p.sw), p.sb);
   Sync sy{mbar, 0u, p.status, STATUS_SURROGATE_WAIT, true};
   uint32_t tmem = 0, trow = 0;
@@ -418,6 +419,8 @@ __global__ void __launch_bounds__(kMaterialThreads, 2) k_material_surrogate(cons
     stage_rowmajor(sW2, w.w2, kMlpHidden, kMlpHidden);
     stage_rowmajor(sW3, w.w3, kMlpHidden, kMlpHidden);
     stage_rowmajor(sW4, w.w4, kMlpOut, kMlpHidden);
+    stage_biases(sBias, w);
+    stage_wait();
     umma::fence_before_sync();
     __syncthreads();
     umma::fence_after_sync();
@@ -455,18 +458,18 @@ __global__ void __launch_bounds__(kMaterialThreads, 2) k_material_surrogate(cons
           st_bf16(sX, t, c, kMlpIn, c < SURROGATE_FEATURES ? f[c] : 0.0f);
         gemm(sy, tmem, sX, sW1, kMlpIn, kMlpHidden);
         if (sy.ok)
-          hidden_epilogue(trow, w.b1, sA, nullptr, nullptr);
+          hidden_epilogue(trow, sBias, sA, nullptr, nullptr);
         gemm(sy, tmem, sA, sW2, kMlpHidden, kMlpHidden);
         if (sy.ok)
-          hidden_epilogue(trow, w.b2, sA, nullptr, nullptr);
+          hidden_epilogue(trow, sBias + kMlpHidden, sA, nullptr, nullptr);
         gemm(sy, tmem, sA, sW3, kMlpHidden, kMlpHidden);
         if (sy.ok)
-          hidden_epilogue(trow, w.b3, sA, nullptr, nullptr);
+          hidden_epilogue(trow, sBias + 2 * kMlpHidden, sA, nullptr, nullptr);
         gemm(sy, tmem, sA, sW4, kMlpHidden, kMlpOut);
         if (sy.ok) {
           float v[16];
           umma::tmem_ld16(trow, v);
-          ratio = v[0] + w.b4[0];
+          ratio = v[0] + sBias[3 * kMlpHidden];
         }
       }
     }

@@ -330,8 +330,9 @@ __global__ void __launch_bounds__(kBondThreads, 2) k_force_tiled(const __grid_co
 // The default bond kernels: kTileP = 2 with the thread's two points held as the two lanes of
 // packed FP32 pairs, so each bond term of both points is one paired instruction (half the
 // arithmetic issue of the scalar kernels above). Windows, masks, operation order and rounding
-// per lane are those of the scalar kernels; a window position that holds a slot of only one
-// point (t = 0: point 0, t = cnt: point 1) runs with the other lane's bond weight zero.
+// per lane are those of the scalar kernels. The window's two ends, each a slot of only one
+// point (t = 0: point 0, t = cnt: point 1), share one pair element in the unrolled windows; the
+// runtime loop runs them as separate elements with the other lane's bond weight zero.
 struct DeformPair {
   float2 jx, jy, jz, ux, uy, uz;  // lane q: point q (jy includes q h)
 };
@@ -361,6 +362,35 @@ __device__ __forceinline__ void deform_pair_element(const StepParams &p, int t, 
   }
 }
 
+// The two ends of a window of CNT slots as one pair: lane 0 takes position 0 (point 0's first
+// slot), lane 1 position CNT (point 1's last slot), each with the operations of
+// deform_pair_element, so a window costs CNT pair elements instead of CNT + 1.
+template <int CNT, bool DAMAGE, typename I>
+__device__ __forceinline__ void deform_pair_ends(const StepParams &p, I j0, I j1, float gx, float gz, float by0,
+                                                 float h, const DeformPair &pt, const uint32_t (&bits)[2],
+                                                 const uint32_t (&live)[2], float2 (&part)[9], uint32_t (&fresh)[2],
+                                                 uint32_t (&near)[2]) {
+  const float4 a0 = ldgf4(p.jit + j0), b0 = ldgf4(p.uf + j0), a1 = ldgf4(p.jit + j1), b1 = ldgf4(p.uf + j1);
+  const float2 e0 = make_float2((a0.x + gx) - pt.jx.x, (a1.x + gx) - pt.jx.y);
+  const float2 e1 = make_float2((a0.y + fmaf(0.0f, h, by0)) - pt.jy.x, (a1.y + fmaf((float)CNT, h, by0)) - pt.jy.y);
+  const float2 e2 = make_float2((a0.z + gz) - pt.jz.x, (a1.z + gz) - pt.jz.y);
+  const float2 d0 = make_float2(b0.x - pt.ux.x, b1.x - pt.ux.y), d1 = make_float2(b0.y - pt.uy.x, b1.y - pt.uy.y);
+  const float2 d2 = make_float2(b0.z - pt.uz.x, b1.z - pt.uz.y);
+  const float2 v = make_float2((bits[0] & 1u) ? a0.w : 0.0f, ((bits[1] >> CNT) & 1u) ? a1.w : 0.0f);
+  const float2 w0 = __fmul2_rn(v, d0), w1 = __fmul2_rn(v, d1), w2 = __fmul2_rn(v, d2);
+  part[0] = __ffma2_rn(w0, e0, part[0]), part[1] = __ffma2_rn(w0, e1, part[1]);
+  part[2] = __ffma2_rn(w0, e2, part[2]), part[3] = __ffma2_rn(w1, e0, part[3]);
+  part[4] = __ffma2_rn(w1, e1, part[4]), part[5] = __ffma2_rn(w1, e2, part[5]);
+  part[6] = __ffma2_rn(w2, e0, part[6]), part[7] = __ffma2_rn(w2, e1, part[7]);
+  part[8] = __ffma2_rn(w2, e2, part[8]);
+  if (DAMAGE) {
+    if (live[0] & 1u)
+      stretch_test(p, 0, e0.x, e1.x, e2.x, d0.x, d1.x, d2.x, fresh[0], near[0]);
+    if ((live[1] >> CNT) & 1u)
+      stretch_test(p, CNT, e0.y, e1.y, e2.y, d0.y, d1.y, d2.y, fresh[1], near[1]);
+  }
+}
+
 template <int CNT, bool DAMAGE, typename I>
 __device__ __forceinline__ void deform_pair_window(const StepParams &p, int cnt, I jb, I nz, I n, float gx, float gz,
                                                    float by0, float h, const DeformPair &pt,
@@ -368,9 +398,11 @@ __device__ __forceinline__ void deform_pair_window(const StepParams &p, int cnt,
                                                    float2 (&part)[9], uint32_t (&fresh)[2], uint32_t (&near)[2]) {
   if constexpr (CNT > 0) {
 #pragma unroll
-    for (int t = 0; t < CNT + 1; ++t)
+    for (int t = 1; t < CNT; ++t)  // positions that hold a slot of both points
       deform_pair_element<DAMAGE, I>(p, t, clamp_to<I>(jb + (I)t * nz, n), gx, gz, by0, h, pt, bits, live, part,
                                      fresh, near);
+    deform_pair_ends<CNT, DAMAGE, I>(p, clamp_to<I>(jb, n), clamp_to<I>(jb + (I)CNT * nz, n), gx, gz, by0, h, pt,
+                                     bits, live, part, fresh, near);
   } else {
     for (int t = 0; t < cnt + 1; ++t)
       deform_pair_element<DAMAGE, I>(p, t, clamp_to<I>(jb + (I)t * nz, n), gx, gz, by0, h, pt, bits, live, part,
@@ -487,14 +519,39 @@ __device__ __forceinline__ void force_pair_element(const StepParams &p, int t, I
   part[2] = __ffma2_rn(m, r2, part[2]);
 }
 
+// The two ends of a window as one pair (lane 0: position 0, lane 1: position CNT), with the
+// operations of force_pair_element.
+template <int CNT, typename I>
+__device__ __forceinline__ void force_pair_ends(const StepParams &p, I j0, I j1, float gx, float gz, float by0,
+                                                float h, const ForcePair &pt, const uint32_t (&bits)[2],
+                                                float2 (&part)[3]) {
+  const float4 *P0 = p.fmapf, *P1 = p.fmapf + p.n, *P2 = p.fmapf + 2 * p.n;
+  const float4 a0 = ldgf4(P0 + j0), b0 = ldgf4(P1 + j0), c0 = ldgf4(P2 + j0);
+  const float4 a1 = ldgf4(P0 + j1), b1 = ldgf4(P1 + j1), c1 = ldgf4(P2 + j1);
+  const float2 e0 = make_float2((a0.w + gx) - pt.jx.x, (a1.w + gx) - pt.jx.y);
+  const float2 e1 = make_float2((b0.w + fmaf(0.0f, h, by0)) - pt.jy.x, (b1.w + fmaf((float)CNT, h, by0)) - pt.jy.y);
+  const float2 e2 = make_float2((c0.w + gz) - pt.jz.x, (c1.w + gz) - pt.jz.y);
+  const float2 m = make_float2((bits[0] & 1u) ? 1.0f : 0.0f, ((bits[1] >> CNT) & 1u) ? 1.0f : 0.0f);
+  const float2 r0 = __ffma2_rn(make_float2(a0.z, a1.z), e2,
+                               __ffma2_rn(make_float2(a0.y, a1.y), e1, __fmul2_rn(make_float2(a0.x, a1.x), e0)));
+  const float2 r1 = __ffma2_rn(make_float2(b0.z, b1.z), e2,
+                               __ffma2_rn(make_float2(b0.y, b1.y), e1, __fmul2_rn(make_float2(b0.x, b1.x), e0)));
+  const float2 r2 = __ffma2_rn(make_float2(c0.z, c1.z), e2,
+                               __ffma2_rn(make_float2(c0.y, c1.y), e1, __fmul2_rn(make_float2(c0.x, c1.x), e0)));
+  part[0] = __ffma2_rn(m, r0, part[0]), part[1] = __ffma2_rn(m, r1, part[1]);
+  part[2] = __ffma2_rn(m, r2, part[2]);
+}
+
 template <int CNT, typename I>
 __device__ __forceinline__ void force_pair_window(const StepParams &p, int cnt, I jb, I nz, I n, float gx, float gz,
                                                   float by0, float h, const ForcePair &pt, const uint32_t (&bits)[2],
                                                   float2 (&part)[3]) {
   if constexpr (CNT > 0) {
 #pragma unroll
-    for (int t = 0; t < CNT + 1; ++t)
+    for (int t = 1; t < CNT; ++t)  // positions that hold a slot of both points
       force_pair_element<I>(p, t, clamp_to<I>(jb + (I)t * nz, n), gx, gz, by0, h, pt, bits, part);
+    force_pair_ends<CNT, I>(p, clamp_to<I>(jb, n), clamp_to<I>(jb + (I)CNT * nz, n), gx, gz, by0, h, pt, bits,
+                            part);
   } else {
     for (int t = 0; t < cnt + 1; ++t)
       force_pair_element<I>(p, t, clamp_to<I>(jb + (I)t * nz, n), gx, gz, by0, h, pt, bits, part);
