@@ -127,6 +127,33 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+# FP32 operations per bond of the mixed bond kernels (the algorithm's, padding slots and
+# masked lanes not counted): deformation xi (3), u_j - u_i (3), V (u_j - u_i) (3), the outer
+# product accumulated (9 FMA = 18); force xi (3), V_j M_j xi (9 FMA = 18, counted as multiply
+# plus add), the accumulation (3).
+FP32_FLOP_PER_BOND = {"deformation": 27, "force": 24}
+FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # 148 SMs x 128 FP32 lanes x FMA at 1965 MHz
+LIMITER = {
+    "deformation": "FP32 issue: FMA pipe 50 %, issue 54 % active, 76 B/pt DRAM "
+                   "(profiles/bond_kernels_pair_and_fp64_tiled_250k.md)",
+    "force": "FP32 issue and L1 gathers: issue 52 % active, FMA pipe 38 %, L1 60 %, 140 B/pt DRAM "
+             "(profiles/bond_kernels_pair_and_fp64_tiled_250k.md)",
+    "material": "FP64 latency at low occupancy (profiles/material_kernels_plastic_and_fp64.md)",
+}
+
+
+def fp32_roofline(kernel, bonds, ms):
+    """The bond kernels are bound by FP32 issue, not HBM: their algorithmic FP32 rate against the
+    nominal FP32 CUDA-core peak (no measured FP32 figure exists for this pool)."""
+    out = {"limiter": LIMITER.get(kernel, "")}
+    if kernel in FP32_FLOP_PER_BOND:
+        tf = bonds * FP32_FLOP_PER_BOND[kernel] / (ms * 1e-3) / 1e12
+        out["fp32"] = {"achieved_tflops": tf, "nominal_peak_tflops": FP32_NOMINAL_TFLOPS,
+                       "frac_of_nominal": tf / FP32_NOMINAL_TFLOPS,
+                       "flop_per_bond": FP32_FLOP_PER_BOND[kernel]}
+    return out
+
+
 def algorithmic_bytes(nw, damage, mixed):
     """Bytes each kernel must move per point per increment: every per-point array it reads or
     writes once, plus the bond bit masks (nw 32-bit words per point; the broken-bond words are
@@ -350,7 +377,8 @@ def run_gpu(args, world, rank, local):
                                **{k: v for k, v in report.items() if k != "epoch_loss"}},
         "roofline": {"kernel": dominant, "bound": "hbm", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
-                     "traffic": tr, "algorithmic_bytes": alg[dominant] * n},
+                     "traffic": tr, "algorithmic_bytes": alg[dominant] * n,
+                     **fp32_roofline(dominant, nb * n, stages[dominant])},
         "step_roofline": {"algorithmic_bytes": step_alg,
                           "achieved_gbs": step_alg / (ms_step * 1e-3) / 1e9,
                           "frac": step_alg / (ms_step * 1e-3) / 1e9 / peak,

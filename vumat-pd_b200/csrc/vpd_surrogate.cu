@@ -4,13 +4,16 @@
 //                          (jc_trial + jc_bisection + jc_finish, the plain path's own code)
 //   train_surrogate        Adam on the weighted MSE, with the tensor-core forward and backward
 //                          kernels of vpd_mlp.cu
-//   k_material_surrogate   the material stage with the network inside: a persistent kernel,
-//                          128 points per tile (thread t = point t = TMEM lane t), weights
-//                          staged once per CTA in shared memory; per tile it runs the
-//                          kinematics and the elastic trial (vpd_material.cuh), the network on
-//                          the tile's yielding points (four tcgen05 products), then per point
-//                          the Newton acceptance (vpd_surrogate.cuh) or the bisection fallback,
-//                          the radial scaling, the force map and the diagnostics partials.
+//   k_material_surrogate   the material stage with the learned return map, 128 points per
+//                          tile: the kinematics and the elastic trial (vpd_material.cuh), the
+//                          network's guess for the points that need it, then per point the
+//                          Newton acceptance (vpd_surrogate.cuh) or the bisection fallback, the
+//                          radial scaling, the force map and the diagnostics partials. With the
+//                          network guess for every yielding point it is a persistent kernel
+//                          with the weights staged once per CTA and the network as four
+//                          tcgen05 products per tile (thread t = point t = TMEM lane t); with
+//                          the hybrid guess the few points without plastic history are
+//                          evaluated by the block on the CUDA cores (sparse_net_ratio).
 #include "vpd_material.cuh"
 #include "vpd_mlp_tile.cuh"
 #include "vpd_surrogate.cuh"
@@ -397,8 +400,71 @@ int train_surrogate(const vpd_surrogate_config &cfg, uint16_t *w_out, float *b_o
 // once the first product has completed) | mbarrier | biases
 constexpr size_t kSurrSmem = 4096 + 32768 + 32768 + 4096 + 32768 + 64 + 4 * kBiasFloats;
 
-template <bool NET>
-__global__ void __launch_bounds__(kMaterialThreads, NET ? 2 : 4) k_material_surrogate(const __grid_constant__ StepParams p) {
+// ------------------------------------------------------------------ sparse network inference
+// The network's plastic-ratio output for ONE point, evaluated by the whole block on the CUDA
+// cores: thread t computes hidden unit t of each layer (the FP32 dot product of its BF16 weight
+// row with the previous layer's BF16 activations, then the bias and SiLU, rounded to BF16 as
+// the tensor-core kernels store it). This serves the hybrid guess, where only the points
+// without plastic history need the network (about 60 of 228k yielding points per increment
+// on the 250k-point bar in plastic flow, in 3 % of the tiles): the material kernel then keeps
+// four blocks per SM, without the 108 KB of staged weights and the TMEM of the tensor-core
+// path. Every thread of the 128-thread block calls it.
+struct SparseNet {
+  float x[16];  // the point's features, BF16-rounded, zero padded
+  float h[2][kMlpHidden];
+  float red[kMaterialThreads / 32];
+};
+
+__device__ __forceinline__ float bf16_lo(uint32_t u) { return __uint_as_float(u << 16); }
+__device__ __forceinline__ float bf16_hi(uint32_t u) { return __uint_as_float(u & 0xffff0000u); }
+__device__ __forceinline__ float bf16_round(float v) { return __bfloat162float(__float2bfloat16(v)); }
+
+// sum_k row[k] in[k] over 8 k8 groups of 8 (row: bf16, 16-byte aligned; in: shared memory)
+__device__ __forceinline__ float dot_bf16_row(const __nv_bfloat16 *row, const float *in, int k8s) {
+  const uint4 *r = reinterpret_cast<const uint4 *>(row);
+  float z = 0.0f;
+#pragma unroll 4
+  for (int k8 = 0; k8 < k8s; ++k8) {
+    const uint4 q = __ldg(r + k8);
+    const float4 a = *reinterpret_cast<const float4 *>(in + 8 * k8);
+    const float4 b = *reinterpret_cast<const float4 *>(in + 8 * k8 + 4);
+    z = fmaf(bf16_lo(q.x), a.x, z), z = fmaf(bf16_hi(q.x), a.y, z);
+    z = fmaf(bf16_lo(q.y), a.z, z), z = fmaf(bf16_hi(q.y), a.w, z);
+    z = fmaf(bf16_lo(q.z), b.x, z), z = fmaf(bf16_hi(q.z), b.y, z);
+    z = fmaf(bf16_lo(q.w), b.z, z), z = fmaf(bf16_hi(q.w), b.w, z);
+  }
+  return z;
+}
+
+__device__ float sparse_net_ratio(const MlpWeights &w, SparseNet &s) {
+  const int t = threadIdx.x;
+  s.h[0][t] = bf16_round(silu(dot_bf16_row(w.w1 + t * kMlpIn, s.x, kMlpIn / 8) + w.b1[t]));
+  __syncthreads();
+  s.h[1][t] = bf16_round(silu(dot_bf16_row(w.w2 + t * kMlpHidden, s.h[0], kMlpHidden / 8) + w.b2[t]));
+  __syncthreads();
+  s.h[0][t] = bf16_round(silu(dot_bf16_row(w.w3 + t * kMlpHidden, s.h[1], kMlpHidden / 8) + w.b3[t]));
+  __syncthreads();
+  float v = __bfloat162float(w.w4[t]) * s.h[0][t];  // output 0: row 0 of W4
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1)
+    v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((t & 31) == 0)
+    s.red[t >> 5] = v;
+  __syncthreads();
+  const float r = (s.red[0] + s.red[1]) + (s.red[2] + s.red[3]) + w.b4[0];
+  __syncthreads();  // s is reused by the next point
+  return r;
+}
+
+// MODE: SURR_WARM (no network), SURR_SPARSE (hybrid guess: sparse_net_ratio for the points
+// without plastic history), SURR_TENSOR (network guess: the tensor-core network on every tile
+// with a yielding point; persistent blocks with the weights staged once).
+enum SurrogateMode { SURR_WARM = 0, SURR_SPARSE = 1, SURR_TENSOR = 2 };
+
+template <int MODE>
+__global__ void __launch_bounds__(kMaterialThreads, MODE == SURR_TENSOR ? 2 : 4)
+    k_material_surrogate(const __grid_constant__ StepParams p) {
+  constexpr bool NET = MODE == SURR_TENSOR;
   extern __shared__ __align__(1024) unsigned char smem[];
   __shared__ uint32_t s_tmem;
   const int t = threadIdx.x;
@@ -450,6 +516,31 @@ __global__ void __launch_bounds__(kMaterialThreads, NET ? 2 : 4) k_material_surr
       }
     }
     float ratio = 0.0f;
+    if (MODE == SURR_SPARSE) {
+      // the tile's points that need the network, one at a time (uniform loop: block votes)
+      __shared__ SparseNet sn;
+      __shared__ int s_who;
+      bool pending = use_net;
+      while (__syncthreads_or(pending)) {
+        if (t == 0)
+          s_who = kMaterialThreads;
+        __syncthreads();
+        if (pending)
+          atomicMin(&s_who, t);
+        __syncthreads();
+        const int who = s_who;
+        if (t == who) {
+          surrogate_features(p.jc, p.dt, m.inc, tr, f);
+#pragma unroll
+          for (int c = 0; c < 16; ++c)
+            sn.x[c] = c < SURROGATE_FEATURES ? bf16_round(f[c]) : 0.0f;
+        }
+        __syncthreads();
+        const float r = sparse_net_ratio(w, sn);
+        if (t == who)
+          ratio = r, pending = false;
+      }
+    }
     if (NET) {
       // the tile's points that need the network (uniform branch: a block-wide vote)
       if (__syncthreads_or(use_net) && sy.ok) {
@@ -506,21 +597,23 @@ int prepare_material_surrogate() {
   int dev = 0;
   VPD_CUDA(cudaGetDevice(&dev));
   VPD_CUDA(cudaDeviceGetAttribute(&g_surrogate_sms, cudaDevAttrMultiProcessorCount, dev));
-  VPD_CUDA(cudaFuncSetAttribute(k_material_surrogate<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  VPD_CUDA(cudaFuncSetAttribute(k_material_surrogate<SURR_TENSOR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)kSurrSmem));
   return VPD_OK;
 }
 
 int launch_material_surrogate(const StepParams &p, cudaStream_t s) {
   const int64_t tiles = (p.n + 127) / 128;
-  if (p.surr_guess != VPD_GUESS_WARM_START) {
+  if (p.surr_guess == VPD_GUESS_NETWORK) {
     if (!g_surrogate_sms)
       return set_error(VPD_ERR_INVALID, "surrogate kernel not prepared (vpd_set_surrogate)");
     // persistent: two CTAs per SM, each staging the weights once
     const int64_t grid = std::min<int64_t>(tiles, 2 * (int64_t)g_surrogate_sms);
-    k_material_surrogate<true><<<(unsigned)grid, kMaterialThreads, kSurrSmem, s>>>(p);
+    k_material_surrogate<SURR_TENSOR><<<(unsigned)grid, kMaterialThreads, kSurrSmem, s>>>(p);
+  } else if (p.surr_guess == VPD_GUESS_HYBRID) {
+    k_material_surrogate<SURR_SPARSE><<<(unsigned)tiles, kMaterialThreads, 0, s>>>(p);
   } else {
-    k_material_surrogate<false><<<(unsigned)tiles, kMaterialThreads, 0, s>>>(p);
+    k_material_surrogate<SURR_WARM><<<(unsigned)tiles, kMaterialThreads, 0, s>>>(p);
   }
   VPD_CUDA(cudaGetLastError());
   return VPD_OK;
