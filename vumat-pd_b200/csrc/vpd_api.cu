@@ -228,6 +228,8 @@ struct vpd_handle {
   double *sig = nullptr, *state = nullptr, *eI = nullptr, *eP = nullptr, *Mt = nullptr, *obsw = nullptr;
   StencilLayout st;
   double *part_mat = nullptr, *part_force = nullptr, *accum = nullptr, *diag = nullptr;
+  double *part_group = nullptr;
+  unsigned *group_counter = nullptr;
   uint8_t *flags = nullptr;
   unsigned *status_dev = nullptr, *counter = nullptr;
   uint16_t *surr_w = nullptr;  // surrogate network (device copies)
@@ -406,9 +408,13 @@ int create_impl(vpd_handle *h, const vpd_case *c, const double *positions, const
   }
   const int mat_blocks = material_grid(n);
   const int force_blocks = integrate_grid(n);
+  const int groups = (force_blocks + kGroupBlocks - 1) / kGroupBlocks;
   if ((rc = dalloc(h, &h->part_mat, (size_t)mat_blocks * PM_COUNT)) ||
-      (rc = dalloc(h, &h->part_force, (size_t)force_blocks * PF_COUNT)))
+      (rc = dalloc(h, &h->part_force, (size_t)force_blocks * PF_COUNT)) ||
+      (rc = dalloc(h, &h->part_group, (size_t)groups * (PM_COUNT + PF_COUNT))) ||
+      (rc = dalloc(h, &h->group_counter, (size_t)groups)))
     return rc;
+  VPD_CUDA(cudaMemsetAsync(h->group_counter, 0, sizeof(unsigned) * groups, s));
 
   // step parameters
   StepParams &p = h->params;
@@ -458,6 +464,7 @@ int create_impl(vpd_handle *h, const vpd_case *c, const double *positions, const
   }
   p.step = h->step_dev, p.status = h->status_dev;
   p.part_mat = h->part_mat, p.part_force = h->part_force, p.accum = h->accum, p.diag = h->diag;
+  p.part_group = h->part_group, p.group_counter = h->group_counter;
   p.counter = h->counter;
   p.mat_blocks = mat_blocks;
   p.interior = sets.interior, p.gauge = sets.gauge, p.lat_gauge = sets.lat_gauge;

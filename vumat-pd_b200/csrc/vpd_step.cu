@@ -16,8 +16,9 @@
 // index loads are coalesced and the bond loop runs to the slice width with the tail masked.
 // The increment number lives in device memory (*step), so the launch sequence is
 // independent of the host and can be captured in a CUDA graph. Diagnostics are reduced
-// deterministically: each block writes a partial, the last block of k_integrate sums them in
-// block order and writes the increment's row.
+// deterministically: each block writes a partial, the last block of each group of k_integrate
+// blocks sums its group's share, and the last group sums the groups in order and writes the
+// increment's row.
 #include "vpd_math.cuh"
 #include "vpd_material.cuh"
 #include "vpd_step.cuh"
@@ -237,7 +238,7 @@ __global__ void __launch_bounds__(kBondThreads) k_force(StepParams p) {
 // ------------------------------------------------------------------ k_integrate
 // Velocity-Verlet correction with the force density, constraints at t_n, diagnostics, then
 // the next increment's prediction with constraints at t_n+1; the last block writes the row.
-__global__ void __launch_bounds__(kBondThreads) k_integrate(StepParams p) {
+__global__ void __launch_bounds__(kBondThreads, 3) k_integrate(StepParams p) {
   const int64_t n = p.n;
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t step = *p.step;
@@ -295,34 +296,42 @@ __global__ void __launch_bounds__(kBondThreads) k_integrate(StepParams p) {
   }
   block_partials<PF_COUNT>(part, p.part_force, blockIdx.x);
 
-  // last block: reduce every block's partials in block order and write the diagnostic row
+  // Two-level reduction, deterministic: the last block of each group of kGroupBlocks blocks sums
+  // the group's force partials and its share of the material partials (each thread its slots in
+  // slot order, then a fixed tree); the last group to finish sums the group partials in group
+  // order and writes the diagnostic row. Every slot is read by one thread of one block, so the
+  // reads run in parallel instead of one block walking all of them.
+  constexpr int Q = PM_COUNT + PF_COUNT;
+  const int ngroups = (int)((gridDim.x + kGroupBlocks - 1) / kGroupBlocks);
+  const int g = (int)(blockIdx.x / kGroupBlocks), gfirst = g * kGroupBlocks;
+  const int gcount = min(kGroupBlocks, (int)gridDim.x - gfirst);
   __shared__ bool last;
   __threadfence();
   if (threadIdx.x == 0)
-    last = atomicAdd(p.counter, 1u) == gridDim.x - 1;
+    last = atomicAdd(p.group_counter + g, 1u) == (unsigned)gcount - 1u;
   __syncthreads();
   if (!last)
     return;
-  // every thread folds a fixed strided subset of the block partials, then a fixed-order tree
-  // over the threads: deterministic, and the partial loads are spread over the whole block
-  double acc[PM_COUNT + PF_COUNT];
+  double acc[Q];
 #pragma unroll
-  for (int q = 0; q < PM_COUNT + PF_COUNT; ++q)
+  for (int q = 0; q < Q; ++q)
     acc[q] = 0.0;
-  for (int b = threadIdx.x; b < p.mat_blocks; b += blockDim.x)
+  const int ms = (p.mat_blocks + ngroups - 1) / ngroups;
+  const int mlo = g * ms, mhi = min(p.mat_blocks, mlo + ms);
+  for (int b = mlo + (int)threadIdx.x; b < mhi; b += blockDim.x)
 #pragma unroll
     for (int q = 0; q < PM_COUNT; ++q) {
       const double v = __ldcg(p.part_mat + (size_t)b * PM_COUNT + q);
       acc[q] = q == PM_MAX_EQPS ? fmax(acc[q], v) : acc[q] + v;
     }
-  for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x)
+  for (int b = gfirst + (int)threadIdx.x; b < gfirst + gcount; b += blockDim.x)
 #pragma unroll
     for (int q = 0; q < PF_COUNT; ++q)
       acc[PM_COUNT + q] += __ldcg(p.part_force + (size_t)b * PF_COUNT + q);
-  __shared__ double red[kBondThreads / 32][PM_COUNT + PF_COUNT];
-  __shared__ double tot[PM_COUNT + PF_COUNT];
+  __shared__ double red[kBondThreads / 32][Q];
+  __shared__ double tot[Q];
 #pragma unroll
-  for (int q = 0; q < PM_COUNT + PF_COUNT; ++q)
+  for (int q = 0; q < Q; ++q)
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
       const double y = __shfl_xor_sync(0xffffffffu, acc[q], o);
@@ -330,14 +339,33 @@ __global__ void __launch_bounds__(kBondThreads) k_integrate(StepParams p) {
     }
   if ((threadIdx.x & 31) == 0)
 #pragma unroll
-    for (int q = 0; q < PM_COUNT + PF_COUNT; ++q)
+    for (int q = 0; q < Q; ++q)
       red[threadIdx.x >> 5][q] = acc[q];
   __syncthreads();
-  if (threadIdx.x < PM_COUNT + PF_COUNT) {
+  if (threadIdx.x < Q) {
     const int q = threadIdx.x;
     double s = 0.0;
     for (int w = 0; w < (int)(blockDim.x >> 5); ++w)
       s = q == PM_MAX_EQPS ? fmax(s, red[w][q]) : s + red[w][q];
+    p.part_group[(size_t)g * Q + q] = s;
+  }
+  if (threadIdx.x == 0)
+    p.group_counter[g] = 0u;  // ready for the next increment
+  __shared__ bool final_group;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0)
+    final_group = atomicAdd(p.counter, 1u) == (unsigned)ngroups - 1u;
+  __syncthreads();
+  if (!final_group)
+    return;
+  if (threadIdx.x < Q) {
+    const int q = threadIdx.x;
+    double s = 0.0;
+    for (int gg = 0; gg < ngroups; ++gg) {
+      const double v = __ldcg(p.part_group + (size_t)gg * Q + q);
+      s = q == PM_MAX_EQPS ? fmax(s, v) : s + v;
+    }
     tot[q] = s;
   }
   __syncthreads();

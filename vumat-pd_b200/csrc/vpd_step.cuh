@@ -22,6 +22,7 @@ enum {
 enum { ACC_INTERNAL = 0, ACC_EXTERNAL, ACC_PREV_POWER, ACC_FINITE, ACC_COUNT };
 
 constexpr int kDiagRing = 4096;      // diagnostic rows buffered on the device
+constexpr int kGroupBlocks = 256;   // k_integrate blocks reduced together by the group's last block
 constexpr int kBondThreads = 256;    // threads per block of the bond kernels
 constexpr int kMaterialThreads = 128;
 constexpr int kMaxStencilWords = 32; // at most 1024 lattice offsets per stencil
@@ -89,7 +90,9 @@ struct StepParams {
   int64_t *step;              // increment being computed (1-based)
   unsigned int *status;
   double *part_mat, *part_force, *accum, *diag;
-  unsigned int *counter;
+  double *part_group;          // per group of kGroupBlocks integrate blocks: PM_COUNT + PF_COUNT sums
+  unsigned int *counter;       // groups done (k_integrate)
+  unsigned int *group_counter; // blocks done, per group
   int mat_blocks;
   // diagnostic constants
   double interior, gauge, lat_gauge, area, sign, n_lat_pos, n_lat_neg;

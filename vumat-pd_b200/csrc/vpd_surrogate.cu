@@ -456,6 +456,52 @@ __device__ float sparse_net_ratio(const MlpWeights &w, SparseNet &s) {
   return r;
 }
 
+struct SurrogateInput {
+  float f[SURROGATE_FEATURES];
+};
+
+struct StrainIncrement {
+  double v[6];
+};
+
+// surrogate_features, out of line with its inputs by value (see sparse_network_guesses).
+__device__ __noinline__ SurrogateInput features_out_of_line(JcParams jc, double dt, StrainIncrement inc,
+                                                             JcTrial tr) {
+  SurrogateInput in;
+  surrogate_features(jc, dt, inc.v, tr, in.f);
+  return in;
+}
+
+// The network guesses of the block's points that need one (pending), one point at a time;
+// returns the calling thread's (0 where it needs none). Every thread of the block calls it. Kept
+// out of line: it runs in few tiles, and inlined its registers would raise the whole kernel's.
+__device__ __noinline__ float sparse_network_guesses(const uint16_t *sw, const float *sb, SurrogateInput in,
+                                                     bool pending) {
+  __shared__ SparseNet sn;
+  __shared__ int s_who;
+  const MlpWeights w = mlp_weights(reinterpret_cast<const __nv_bfloat16 *>(sw), sb);
+  const int t = threadIdx.x;
+  float ratio = 0.0f;
+  while (__syncthreads_or(pending)) {
+    if (t == 0)
+      s_who = kMaterialThreads;
+    __syncthreads();
+    if (pending)
+      atomicMin(&s_who, t);
+    __syncthreads();
+    const int who = s_who;
+    if (t == who)
+#pragma unroll
+      for (int c = 0; c < 16; ++c)
+        sn.x[c] = c < SURROGATE_FEATURES ? bf16_round(in.f[c]) : 0.0f;
+    __syncthreads();
+    const float r = sparse_net_ratio(w, sn);
+    if (t == who)
+      ratio = r, pending = false;
+  }
+  return ratio;
+}
+
 // MODE: SURR_WARM (no network), SURR_SPARSE (hybrid guess: sparse_net_ratio for the points
 // without plastic history), SURR_TENSOR (network guess: the tensor-core network on every tile
 // with a yielding point; persistent blocks with the weights staged once).
@@ -516,30 +562,13 @@ __global__ void __launch_bounds__(kMaterialThreads, MODE == SURR_TENSOR ? 2 : 4)
       }
     }
     float ratio = 0.0f;
-    if (MODE == SURR_SPARSE) {
-      // the tile's points that need the network, one at a time (uniform loop: block votes)
-      __shared__ SparseNet sn;
-      __shared__ int s_who;
-      bool pending = use_net;
-      while (__syncthreads_or(pending)) {
-        if (t == 0)
-          s_who = kMaterialThreads;
-        __syncthreads();
-        if (pending)
-          atomicMin(&s_who, t);
-        __syncthreads();
-        const int who = s_who;
-        if (t == who) {
-          surrogate_features(p.jc, p.dt, m.inc, tr, f);
-#pragma unroll
-          for (int c = 0; c < 16; ++c)
-            sn.x[c] = c < SURROGATE_FEATURES ? bf16_round(f[c]) : 0.0f;
-        }
-        __syncthreads();
-        const float r = sparse_net_ratio(w, sn);
-        if (t == who)
-          ratio = r, pending = false;
-      }
+    if (MODE == SURR_SPARSE && __syncthreads_or(use_net)) {  // block-uniform, 3 % of the tiles
+      SurrogateInput in{};
+      if (use_net)
+        in = features_out_of_line(p.jc, p.dt, StrainIncrement{{m.inc[0], m.inc[1], m.inc[2], m.inc[3], m.inc[4],
+                                                                m.inc[5]}},
+                                  tr);
+      ratio = sparse_network_guesses(p.sw, p.sb, in, use_net);
     }
     if (NET) {
       // the tile's points that need the network (uniform branch: a block-wide vote)
