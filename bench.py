@@ -136,7 +136,7 @@ FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # 148 SMs x 128 FP32 lanes
 LIMITER = {
     "deformation": "FP32 issue: FMA pipe 50 %, issue 54 % active, 76 B/pt DRAM "
                    "(profiles/bond_kernels_pair_and_fp64_tiled_250k.md)",
-    "force": "FP32 issue and L1 gathers: issue 52 % active, FMA pipe 38 %, L1 60 %, 140 B/pt DRAM "
+    "force": "FP32 issue and L1 gathers: issue 59 % active, FMA pipe 41 %, L1 69 %, 140 B/pt DRAM "
              "(profiles/bond_kernels_pair_and_fp64_tiled_250k.md)",
     "material": "FP64 latency at low occupancy (profiles/material_kernels_plastic_and_fp64.md)",
 }
