@@ -455,11 +455,17 @@ int create_impl(vpd_handle *h, const vpd_case *c, const double *positions, const
     if (!h->st.nw)
       return set_error(VPD_ERR_UNSUPPORTED,
                        "mixed precision needs the points in lattice order (lattice-stencil bonds)");
-    float4 *jit = nullptr;
-    if ((rc = dalloc(h, &jit, n)) || (rc = dalloc(h, &p.uf, n)) || (rc = dalloc(h, &p.Gf, 9 * n)) ||
-        (rc = dalloc(h, &p.fmapf, 3 * n)))
+    // neighbour records with zero halos (StepParams): the packed bond kernels' window loads
+    // stay in bounds without clamping, and a masked-out lane reads finite zeros
+    const int64_t H = h->st.halo;
+    float4 *jit = nullptr, *uf = nullptr, *fmapf = nullptr;
+    if ((rc = dalloc(h, &jit, n + 2 * H)) || (rc = dalloc(h, &uf, n + 2 * H)) || (rc = dalloc(h, &p.Gf, 9 * n)) ||
+        (rc = dalloc(h, &fmapf, 3 * n + 2 * H)))
       return rc;
-    p.jit = jit;
+    VPD_CUDA(cudaMemsetAsync(jit, 0, sizeof(float4) * (n + 2 * H), s));
+    VPD_CUDA(cudaMemsetAsync(uf, 0, sizeof(float4) * (n + 2 * H), s));
+    VPD_CUDA(cudaMemsetAsync(fmapf, 0, sizeof(float4) * (3 * n + 2 * H), s));
+    p.jit = jit + H, p.uf = uf + H, p.fmapf = fmapf + H;
     p.mixed = 1;
   }
   p.step = h->step_dev, p.status = h->status_dev;

@@ -37,6 +37,7 @@ struct StencilLayout {
   uint32_t *mask = nullptr;    // [nw][n] bond bits
   uint32_t *broken = nullptr;  // [nw][n] broken-bond bits
   float4 *e0 = nullptr;        // [32 nw] lattice offset of each slot times h (mixed precision)
+  int64_t halo = 0;            // points a tile's window can reach beyond either end of the lattice
 };
 
 struct StepParams {
@@ -66,6 +67,8 @@ struct StepParams {
   double4 *vxi;               // sum over all bonds of V_j xi (FP64, set once; stencil layout)
   // mixed precision (VPD_PRECISION_MIXED): FP32 copies gathered by the bond kernels
   int mixed;
+  // mixed precision: jit, uf and fmapf carry st.halo zero records before and after their n
+  // (3n) records, so the packed bond kernels read window neighbours unclamped
   float4 *jit;                // (X_i - lattice position, V_i)
   float4 *uf;                 // predicted displacement
   float *Gf;                  // sum V_j (u_j - u_i) (x) xi, 9 floats structure of arrays

@@ -330,7 +330,9 @@ __global__ void __launch_bounds__(kBondThreads, 2) k_force_tiled(const __grid_co
 // The default bond kernels: kTileP = 2 with the thread's two points held as the two lanes of
 // packed FP32 pairs, so each bond term of both points is one paired instruction (half the
 // arithmetic issue of the scalar kernels above). Windows, masks, operation order and rounding
-// per lane are those of the scalar kernels. The window's two ends, each a slot of only one
+// per lane are those of the scalar kernels; the unrolled windows index their neighbours without
+// clamping (the neighbour arrays carry zero halos as deep as a window reaches, st.halo). The
+// window's two ends, each a slot of only one
 // point (t = 0: point 0, t = cnt: point 1), share one pair element in the unrolled windows; the
 // runtime loop runs them as separate elements with the other lane's bond weight zero.
 struct DeformPair {
@@ -398,11 +400,9 @@ __device__ __forceinline__ void deform_pair_window(const StepParams &p, int cnt,
                                                    float2 (&part)[9], uint32_t (&fresh)[2], uint32_t (&near)[2]) {
   if constexpr (CNT > 0) {
 #pragma unroll
-    for (int t = 1; t < CNT; ++t)  // positions that hold a slot of both points
-      deform_pair_element<DAMAGE, I>(p, t, clamp_to<I>(jb + (I)t * nz, n), gx, gz, by0, h, pt, bits, live, part,
-                                     fresh, near);
-    deform_pair_ends<CNT, DAMAGE, I>(p, clamp_to<I>(jb, n), clamp_to<I>(jb + (I)CNT * nz, n), gx, gz, by0, h, pt,
-                                     bits, live, part, fresh, near);
+    for (int t = 1; t < CNT; ++t)  // positions that hold a slot of both points (unclamped: halo)
+      deform_pair_element<DAMAGE, I>(p, t, jb + (I)t * nz, gx, gz, by0, h, pt, bits, live, part, fresh, near);
+    deform_pair_ends<CNT, DAMAGE, I>(p, jb, jb + (I)CNT * nz, gx, gz, by0, h, pt, bits, live, part, fresh, near);
   } else {
     for (int t = 0; t < cnt + 1; ++t)
       deform_pair_element<DAMAGE, I>(p, t, clamp_to<I>(jb + (I)t * nz, n), gx, gz, by0, h, pt, bits, live, part,
@@ -548,10 +548,9 @@ __device__ __forceinline__ void force_pair_window(const StepParams &p, int cnt, 
                                                   float2 (&part)[3]) {
   if constexpr (CNT > 0) {
 #pragma unroll
-    for (int t = 1; t < CNT; ++t)  // positions that hold a slot of both points
-      force_pair_element<I>(p, t, clamp_to<I>(jb + (I)t * nz, n), gx, gz, by0, h, pt, bits, part);
-    force_pair_ends<CNT, I>(p, clamp_to<I>(jb, n), clamp_to<I>(jb + (I)CNT * nz, n), gx, gz, by0, h, pt, bits,
-                            part);
+    for (int t = 1; t < CNT; ++t)  // positions that hold a slot of both points (unclamped: halo)
+      force_pair_element<I>(p, t, jb + (I)t * nz, gx, gz, by0, h, pt, bits, part);
+    force_pair_ends<CNT, I>(p, jb, jb + (I)CNT * nz, gx, gz, by0, h, pt, bits, part);
   } else {
     for (int t = 0; t < cnt + 1; ++t)
       force_pair_element<I>(p, t, clamp_to<I>(jb + (I)t * nz, n), gx, gz, by0, h, pt, bits, part);
