@@ -654,8 +654,9 @@ __global__ void __launch_bounds__(kBondThreads, 3) k_force_pair(const __grid_con
 }
 
 // ------------------------------------------------------------------ launchers
-// With damage the deformation kernels keep the runtime window loop: unrolled, the stretch
-// tests made the scalar kernel slower (0.28 against 0.25 ms on the 250k-point bar).
+// With damage the scalar deformation kernel keeps the runtime window loop (unrolled, its
+// stretch tests made it slower: 0.28 against 0.25 ms on the 250k-point bar); the packed-pair
+// kernel unrolls its windows with damage too (0.72 against 0.75 ms on the 1M-point bar).
 template <bool UNROLL> static void launch_deformation(const StepParams &p, cudaStream_t s) {
   const unsigned grid = tiled_grid<2>(p);
   if (p.tiled == 1) {
@@ -665,7 +666,7 @@ template <bool UNROLL> static void launch_deformation(const StepParams &p, cudaS
       k_deformation_tiled<false, 2, UNROLL><<<grid, kBondThreads, 0, s>>>(p);
   } else {
     if (p.damage)
-      k_deformation_pair<true, false><<<grid, kBondThreads, 0, s>>>(p);
+      k_deformation_pair<true, UNROLL><<<grid, kBondThreads, 0, s>>>(p);
     else
       k_deformation_pair<false, UNROLL><<<grid, kBondThreads, 0, s>>>(p);
   }
