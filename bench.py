@@ -134,9 +134,9 @@ class ClockSampler:
 FP32_FLOP_PER_BOND = {"deformation": 27, "force": 24}
 FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # 148 SMs x 128 FP32 lanes x FMA at 1965 MHz
 LIMITER = {
-    "deformation": "FP32 issue: FMA pipe 50 %, issue 54 % active, 76 B/pt DRAM "
+    "deformation": "FP32 issue: FMA pipe 52 % and throttling, issue 51 % active, 76 B/pt DRAM "
                    "(profiles/bond_kernels_pair_and_fp64_tiled_250k.md)",
-    "force": "FP32 issue and L1 gathers: issue 59 % active, FMA pipe 41 %, L1 69 %, 140 B/pt DRAM "
+    "force": "FP32 issue and L1 gathers: issue 57 % active, FMA pipe 42 %, L1 71 %, 140 B/pt DRAM "
              "(profiles/bond_kernels_pair_and_fp64_tiled_250k.md)",
     "material": "FP64 latency at low occupancy (profiles/material_kernels_plastic_and_fp64.md)",
 }
