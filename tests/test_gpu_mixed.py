@@ -57,6 +57,25 @@ def test_mixed_damage_decisions_match_fp64_early():
     assert nrmse(r32[:, STRESS], r64[:, STRESS]) < TOL
 
 
+def test_thin_lattice_windows_reach_past_both_ends(monkeypatch):
+    """A lattice thinner than the stencil (8 x 3 x 5 points, horizon 4.015 h, jittered): the
+    packed kernels' windows reach several planes past every end of the lattice, into the zero
+    halos of their neighbour arrays, while the per-slot kernels clamp every index. Both must
+    give the same increments to FP32 rounding, and the mixed run must track FP64."""
+    case = tensile_bar(3, nx=8, ny=3, nz=5, damage_mode=0, precision=PRECISION_MIXED)
+    monkeypatch.setenv("VPD_BOND_KERNEL", "slot")
+    rs, us, _, _ = run(case, 300)
+    monkeypatch.setenv("VPD_BOND_KERNEL", "pair")
+    rp, up, _, _ = run(case, 300)
+    assert np.all(np.isfinite(rp)) and np.all(np.isfinite(up))
+    assert nrmse(rp[:, STRESS], rs[:, STRESS]) < 1e-5
+    assert nrmse(up, us) < 1e-5
+    monkeypatch.delenv("VPD_BOND_KERNEL")
+    r64, u64, _, _ = run(case.replace(precision=PRECISION_FP64), 300)
+    assert nrmse(rp[:, STRESS], r64[:, STRESS]) < 1e-4
+    assert nrmse(up, u64) < 1e-4
+
+
 def test_mixed_requires_lattice_layout(monkeypatch):
     monkeypatch.setenv("VPD_BOND_LAYOUT", "ell")
     with pytest.raises(vpd.VpdError) as e:
