@@ -436,15 +436,23 @@ __global__ void __launch_bounds__(kBondThreads, 2) k_deformation_pair(const __gr
 #pragma unroll
   for (int c = 0; c < 9; ++c)
     G[c] = make_float2(0.0f, 0.0f);
+  int word = -1;  // the mask word held in mw (groups come in slot order: several per word)
+  uint32_t mw[2] = {0u, 0u};
   for (int g = 0; g < p.st.ngroups; ++g) {
     const int4 gr = __ldg(p.st.groups + g);  // dx, dz, lowest dy, (slots << 16) | first slot
     const int cnt = gr.w >> 16, pos = gr.w & 0xffff, wd = pos >> 5, sh = pos & 31;
     const uint32_t cm = cnt >= 32 ? ~0u : ((1u << cnt) - 1u);
+    if (wd != word) {  // uniform: the group table is the same for every thread
+      word = wd;
+#pragma unroll
+      for (int q = 0; q < 2; ++q)
+        mw[q] = vp[q] ? __ldg(p.st.mask + (int64_t)wd * n + ip[q]) : 0u;
+    }
     uint32_t bits[2], live[2];
     const uint32_t fw = DAMAGE ? group_bits(__ldg(p.st.forward + wd), sh, cm) : 0u;
 #pragma unroll
     for (int q = 0; q < 2; ++q) {
-      const uint32_t m = vp[q] ? group_bits(__ldg(p.st.mask + (int64_t)wd * n + ip[q]), sh, cm) : 0u;
+      const uint32_t m = group_bits(mw[q], sh, cm);
       bits[q] = m << q;  // bit t: the neighbour at window position t (slot pos + t - q)
       live[q] = 0u;
       if (DAMAGE) {
@@ -587,14 +595,22 @@ __global__ void __launch_bounds__(kBondThreads, 3) k_force_pair(const __grid_con
 #pragma unroll
   for (int c = 0; c < 3; ++c)
     fs[c] = fc[c] = make_float2(0.0f, 0.0f), corr[0][c] = corr[1][c] = 0.0;
+  int word = -1;  // the mask word held in mw (groups come in slot order: several per word)
+  uint32_t mw[2] = {0u, 0u};
   for (int g = 0; g < p.st.ngroups; ++g) {
     const int4 gr = __ldg(p.st.groups + g);
     const int cnt = gr.w >> 16, pos = gr.w & 0xffff, wd = pos >> 5, sh = pos & 31;
     const uint32_t cm = cnt >= 32 ? ~0u : ((1u << cnt) - 1u);
+    if (wd != word) {  // uniform: the group table is the same for every thread
+      word = wd;
+#pragma unroll
+      for (int q = 0; q < 2; ++q)
+        mw[q] = vp[q] ? __ldg(p.st.mask + (int64_t)wd * n + ip[q]) : 0u;
+    }
     uint32_t bits[2];
 #pragma unroll
     for (int q = 0; q < 2; ++q) {
-      uint32_t m = vp[q] ? group_bits(__ldg(p.st.mask + (int64_t)wd * n + ip[q]), sh, cm) : 0u;
+      uint32_t m = group_bits(mw[q], sh, cm);
       if (p.damage && m) {
         const uint32_t bk = m & group_bits(p.st.broken[(int64_t)wd * n + ip[q]], sh, cm);
         for (uint32_t f = bk; f; f &= f - 1) {  // broken bonds leave s_i
