@@ -34,6 +34,7 @@ Printed JSON line (rank 0):
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import os
 import statistics
@@ -186,6 +187,24 @@ def algorithmic_bytes(nw, damage, mixed):
     }
 
 
+# FP64 operations per particle-step of the plain path (the F pass, the force pass and the
+# point-wise work, counted as the algorithm's, about 75 per bond) and the nominal FP64 peak:
+# 148 SMs x 64 FP64 FMA lanes x 2 at 1965 MHz.
+FP64_FLOP_PER_BOND = 75
+FP64_NOMINAL_TFLOPS = 148 * 64 * 2 * 1.965e9 / 1e12
+
+
+def plain_roofline(n, nb, ms, peak_gbs):
+    """The plain FP64 path against both of its ceilings: the index formulation's bytes at the
+    measured HBM bandwidth, and its algorithmic FP64 operations at the nominal FP64 peak."""
+    bytes_ = survey_bytes(nb, False) * n
+    tf = FP64_FLOP_PER_BOND * nb * n / (ms * 1e-3) / 1e12
+    return {"ms_per_step": ms, "index_formulation_bytes": bytes_,
+            "index_formulation_frac": bytes_ / (ms * 1e-3) / 1e9 / peak_gbs,
+            "fp64_flop_per_particle_step": FP64_FLOP_PER_BOND * nb, "achieved_fp64_tflops": tf,
+            "nominal_fp64_peak_tflops": FP64_NOMINAL_TFLOPS, "fp64_frac_of_nominal": tf / FP64_NOMINAL_TFLOPS}
+
+
 def survey_bytes(nb, damage):
     """The per-particle-step figure of the index-based formulation: 1264 + 8 nb bytes (+0.25 nb
     with damage), i.e. the per-point state plus one 4-byte index per bond in each bond pass."""
@@ -214,12 +233,24 @@ def cpu_reference(steps, warmup):
     dt = time.perf_counter() - t0
     n = sim.n_points
     stages = sim.stage_seconds()
-    sim.close()
     cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    # one thread on the same run (the library's OpenMP runtime is this process's libgomp)
+    single = None
+    try:
+        gomp = ctypes.CDLL("libgomp.so.1")
+        gomp.omp_set_num_threads(1)
+        t1 = time.perf_counter()
+        sim.step(1)
+        single = n / (time.perf_counter() - t1)
+        gomp.omp_set_num_threads(cores)
+    except OSError:
+        pass
+    sim.close()
     return {"value": n * steps / dt, "unit": UNIT, "cores": cores, "kind": "reference",
             "sample": f"{SAMPLE_NX}x50x50 slab of the bar ({n} points, same horizon, jitter, "
                       f"damage), increments {warmup + 1}-{warmup + steps} from rest",
-            "stage_seconds": {k: round(v, 3) for k, v in stages.items()}}
+            "stage_seconds": {k: round(v, 3) for k, v in stages.items()},
+            "one_thread_value": single}
 
 
 def run_reference(args, world, rank):
@@ -233,7 +264,8 @@ def run_reference(args, world, rank):
         "dtype": "f64", "data": "synthetic",
         "config": {"workload": "tensile_bar_3 (400x50x50 jittered steel JC bar), CPU sample",
                    "sample": base["sample"]},
-        "cpu_baseline": {k: base[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "cpu_baseline": {k: base[k] for k in ("value", "unit", "cores", "kind", "sample", "stage_seconds",
+                                              "one_thread_value")},
         "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }), flush=True)
@@ -384,7 +416,9 @@ def run_gpu(args, world, rank, local):
                           "frac": step_alg / (ms_step * 1e-3) / 1e9 / peak,
                           "index_formulation_bytes": survey,
                           "index_formulation_frac": survey / (ms_step * 1e-3) / 1e9 / peak},
-        "cpu_baseline": {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "cpu_baseline": {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample", "stage_seconds",
+                                             "one_thread_value")},
+        "plain_fp64_roofline": plain_roofline(n, nb, ref["ms_per_step"], peak),
         "e2e": {"value": job_throughput(n, total, e2e_s * 1e3, world), "unit": UNIT,
                 "h2d_bytes_per_step": h2d / total, "d2h_bytes_per_step": d2h / total,
                 "includes": f"vpd_create from host arrays (neighbour search, K^-1), network "
