@@ -18,6 +18,13 @@ Fixtures (read by the tests; nothing at test time reads the reference checkout):
   ref_jc_thermal.npz           one plastic step of the restated JC plugin (pinned bit for bit
                                to the archived run above) with the inputs of the reference's
                                tests/jc_thermal_units_test.cpp, for workToHeat 1 and 1e6
+  cases/*.json                 the reference's case files benchmarks/tensile3d/cases/*.json
+                               (copied), and configs/johnson_cook.json, the material config they
+                               name, under the same relative path
+  pd_coarse_snapshot_head.csv.gz  the header and first 200 rows of the archived
+                               raw/pd_coarse/field_snapshots.csv.gz (its text, for the writer)
+
+`--cases-only` refreshes only the last two.
 """
 import csv
 import gzip
@@ -33,7 +40,25 @@ sys.path.insert(0, os.path.join(ROOT, "oracle"))
 sys.path.insert(0, os.path.join(ROOT, "vumat-pd_b200"))
 
 
+def copy_cases(reference):
+    """The case files, their material config and the head of the archived snapshot file."""
+    src = os.path.join(reference, "benchmarks", "tensile3d", "cases")
+    os.makedirs(os.path.join(HERE, "cases"), exist_ok=True)
+    for name in sorted(os.listdir(src)):
+        if name.endswith(".json"):
+            shutil.copyfile(os.path.join(src, name), os.path.join(HERE, "cases", name))
+    os.makedirs(os.path.join(HERE, "configs"), exist_ok=True)
+    shutil.copyfile(os.path.join(reference, "configs", "johnson_cook.json"),
+                    os.path.join(HERE, "configs", "johnson_cook.json"))
+    raw = os.path.join(reference, "benchmarks", "tensile3d", "raw", "pd_coarse")
+    with gzip.open(os.path.join(raw, "field_snapshots.csv.gz"), "rt") as f:
+        head = [next(f) for _ in range(201)]
+    with gzip.GzipFile(os.path.join(HERE, "pd_coarse_snapshot_head.csv.gz"), "wb", mtime=0) as g:
+        g.write("".join(head).encode())
+
+
 def main(reference):
+    copy_cases(reference)
     import oracle as O
     from vpd.case import Case, REFERENCE_JC_PROPS, tensile_bar
 
@@ -96,4 +121,9 @@ def main(reference):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    args = [a for a in sys.argv[1:] if not a.startswith("--")]
+    ref = args[0] if args else "/root/reference"
+    if "--cases-only" in sys.argv:
+        copy_cases(ref)
+    else:
+        main(ref)

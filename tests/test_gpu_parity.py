@@ -168,6 +168,50 @@ def test_increment_reproduces_archived_pd_coarse():
     assert np.all(mine[:, header.index("finite")] == 1.0)
 
 
+def test_case_file_runner_reproduces_archived_pd_coarse(tmp_path):
+    """The reference's own case file pd_coarse.json run through vpd.runner: the three output
+    files come out in the reference's layout, the timeseries has the archived rows and stress
+    history, the snapshot has the archived points (reference coordinates to the last printed
+    digit) and fields, and the case's acceptance verdict is the archived 'pass'."""
+    import csv
+    import gzip
+    import json
+    from vpd.runner import run_boundary_case
+    rc = run_boundary_case(golden("cases/pd_coarse.json"), str(tmp_path), golden(""), log=lambda line: None)
+    assert rc == 0
+    header, g = load_golden_timeseries()
+    with open(tmp_path / "timeseries.csv") as f:
+        mine = list(csv.reader(f))
+    assert mine[0] == ["material"] + header
+    vals = np.array([[float(x) for x in r[1:]] for r in mine[1:]])
+    assert vals.shape == g.shape and np.array_equal(vals[:, 0], g[:, 0])
+    j = header.index("average_axial_stress_MPa")
+    assert nrmse(vals[:, j], g[:, j]) < 1e-6
+    with open(tmp_path / "field_snapshots.csv") as f:
+        snap = list(csv.reader(f))
+    with gzip.open(golden("pd_coarse_snapshot_head.csv.gz"), "rt") as f:
+        head = list(csv.reader(f))
+    assert snap[0] == head[0] and len(snap) == 1 + 1683
+    for a, b in zip(snap[1:], head[1:]):
+        assert a[:7] == b[:7]  # material, step, time, particle, x0 y0 z0
+    col = {k: i for i, k in enumerate(head[0])}
+    ref = np.load(golden("pd_coarse_snapshot.npz"))
+
+    def arr(*names):
+        return np.array([[float(r[col[k]]) for k in names] for r in snap[1:]])
+
+    assert max_rel(arr("ux_mm", "uy_mm", "uz_mm"), ref["displacement"]) < 1e-9
+    assert max_rel(arr("vx_mm_per_ms", "vy_mm_per_ms", "vz_mm_per_ms"), ref["velocity"]) < 1e-6
+    assert max_rel(arr("axial_stress_MPa")[:, 0], ref["axial_stress"]) < 1e-8
+    assert max_rel(arr("axial_strain")[:, 0], ref["axial_strain"]) < 1e-8
+    assert max_rel(arr("eqps")[:, 0], ref["eqps"]) < 1e-8
+    with open(tmp_path / "metadata.json") as f:
+        meta = json.load(f)
+    assert meta["status"] == "pass" and meta["particles"] == 1683
+    assert meta["materials"][0]["maxEqps"] == pytest.approx(0.0278018224371612, rel=1e-8)
+    assert meta["materials"][0]["finalReaction_N"] == pytest.approx(9875.54163611348, rel=1e-8)
+
+
 def test_increment_matches_reference_library_jittered_damage():
     ref = np.load(golden("ref_tensile_bar_1.npz"))
     bar = tensile_bar(1, jitter=0.05, jitter_seed=7, damage_mode=1, damage_initiation=0.004)

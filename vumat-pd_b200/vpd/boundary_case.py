@@ -1,0 +1,224 @@
+"""The reference's JSON boundary-value cases, read into ``Case`` objects.
+
+``load_boundary_case(path)`` reads a ``vumat_pd_boundary_case`` file (the reference's
+benchmarks/tensile3d/cases/*.json schema, parsed by src/config/DemoConfig.cpp:281-331 with the
+defaults of include/DemoConfig.hpp:13-107) and the material config files it names
+(src/config/MaterialConfigJson.cpp:63-101), and returns a ``BoundaryCase``: one ``Case`` per
+material entry plus what the output files need (labels, output cadence, acceptance limits).
+
+Only what the device increment implements is accepted; anything else raises ``ValueError``
+naming the field:
+  * boundary type ``regional_smooth_displacement`` (half-cosine displacement of the load band,
+    BoundaryConditions.cpp:70-79), loading component x (support ``left``, load ``right``) or
+    y (``bottom``/``top``), rigid-body suppression on;
+  * the Johnson-Cook material (cmname JOHNSONCOOK, 14 props, 6 state variables), corotational
+    stress frame, the legacy_vumat_pd tensor convention, no initial-state overrides or internal
+    indicator;
+  * damage ``none`` or ``critical_stretch``.
+"""
+from __future__ import annotations
+
+import dataclasses
+import json
+import math
+import os
+
+from .case import (BC_SMOOTH_DISPLACEMENT, DAMAGE_CRITICAL_STRETCH, DAMAGE_NONE, Case)
+
+
+@dataclasses.dataclass
+class MaterialRun:
+    """One material entry of a case: its ``Case`` and what its outputs report."""
+    label: str
+    case: Case
+    elastic_e: float                 # for the analytical plane-strain slope E / (1 - nu^2)
+    elastic_nu: float
+    eqps_index: int                  # state variable written as eqps (-1: none)
+    source_density: float            # the material config's density (kg/m^3)
+
+
+@dataclasses.dataclass
+class BoundaryCase:
+    name: str
+    classification: str
+    scope: str
+    steps: int
+    dt: float
+    output_every: int
+    snapshot_every: int              # 0: only the last step
+    component: str                   # "x" or "y"
+    support_region: str
+    load_region: str
+    energy_tolerance: float
+    net_force_tolerance: float
+    minimum_plastic_strain: float
+    kinetic_to_internal_limit: float
+    output_directory: str
+    materials: list
+
+
+def _get(obj, key, default, kind):
+    if key not in obj:
+        return default
+    value = obj[key]
+    if kind is float:
+        if isinstance(value, bool) or not isinstance(value, (int, float)):
+            raise ValueError(f"{key} must be a number")
+        return float(value)
+    if kind is int:
+        if isinstance(value, bool) or not isinstance(value, (int, float)) or int(value) != value:
+            raise ValueError(f"{key} must be an integer")
+        return int(value)
+    if kind is bool:
+        if not isinstance(value, bool):
+            raise ValueError(f"{key} must be true or false")
+        return value
+    if not isinstance(value, str):
+        raise ValueError(f"{key} must be a string")
+    return value
+
+
+def _section(root, key):
+    obj = root.get(key, {})
+    if not isinstance(obj, dict):
+        raise ValueError(f"{key} must be a JSON object")
+    return obj
+
+
+def load_material_config(path: str) -> dict:
+    """A VUMAT material config (configs/*.json), checked against what the device VUMAT runs."""
+    with open(path) as f:
+        root = json.load(f)
+    if _get(root, "schemaVersion", "1.0", str) != "1.0":
+        raise ValueError(f"{path}: unsupported material schemaVersion")
+    cmname = _get(root, "cmname", "", str)
+    if cmname.upper() != "JOHNSONCOOK":
+        raise ValueError(f"{path}: cmname {cmname!r}: only the Johnson-Cook VUMAT runs on the device")
+    if _get(root, "tensorConvention", "legacy_vumat_pd", str) != "legacy_vumat_pd":
+        raise ValueError(f"{path}: tensorConvention must be legacy_vumat_pd")
+    if _get(root, "stressFrame", "corotational", str) != "corotational":
+        raise ValueError(f"{path}: boundary cases need the corotational stress frame")
+    if _get(root, "ndir", 3, int) != 3 or _get(root, "nshr", 3, int) != 3:
+        raise ValueError(f"{path}: ndir and nshr must be 3")
+    nstatev = _get(root, "nstatev", 0, int)
+    props = root.get("props")
+    if not isinstance(props, list) or len(props) != 14 or nstatev != 6:
+        raise ValueError(f"{path}: Johnson-Cook needs 14 props and 6 state variables")
+    density = _get(root, "density", 0.0, float)
+    if density <= 0.0:
+        raise ValueError(f"{path}: density must be positive")
+    return {"props": tuple(float(p) for p in props), "nstatev": nstatev, "density": density}
+
+
+def load_boundary_case(path: str, config_root: str = None) -> BoundaryCase:
+    """Reads a boundary-value case file. Material config paths are resolved against
+    ``config_root`` (default: the current directory, as the reference's host resolves them)."""
+    with open(path) as f:
+        root = json.load(f)
+    if _get(root, "schemaVersion", "1.0", str) != "1.0":
+        raise ValueError("unsupported case schemaVersion")
+    name = _get(root, "name", None, str)
+    if name is None:
+        raise ValueError("the case needs a name")
+    kind = _get(root, "type", "vumat_pd_demo", str)
+    if kind != "vumat_pd_boundary_case":
+        raise ValueError(f"type {kind!r}: only vumat_pd_boundary_case files run here")
+
+    geo = _section(root, "geometry") or _section(root, "grid")
+    if _get(geo, "type", "patch", str) != "patch":
+        raise ValueError("geometry.type must be patch")
+    nx, ny, nz = (_get(geo, k, 1, int) for k in ("nx", "ny", "nz"))
+    spacing = _get(geo, "spacing", 1.0, float)
+    horizon = _get(geo, "horizon", 1.0, float)
+
+    ti = _section(root, "time_integration") or root
+    steps = _get(ti, "steps", 1, int)
+    dt = _get(ti, "dt", 1.0e-6, float)
+
+    bc = _section(root, "boundary_conditions")
+    bc_type = _get(bc, "type", "affine_displacement", str)
+    if bc_type != "regional_smooth_displacement":
+        raise ValueError(f"boundary_conditions.type {bc_type!r}: only regional_smooth_displacement runs here")
+    component = _get(bc, "component", "x", str)
+    support = _get(bc, "supportRegion", "left", str)
+    load = _get(bc, "loadRegion", "right", str)
+    expected = {"x": ("left", "right"), "y": ("bottom", "top")}
+    if component not in expected:
+        raise ValueError(f"boundary_conditions.component {component!r}: x or y")
+    if (support, load) != expected[component]:
+        raise ValueError(f"boundary_conditions: support {support!r} and load {load!r}: the device "
+                         f"increment holds the {expected[component][0]} band and loads the "
+                         f"{expected[component][1]} one")
+    if not _get(bc, "rigidBodySuppression", False, bool):
+        raise ValueError("boundary_conditions.rigidBodySuppression must be true: the device "
+                         "increment always pins the rigid-body modes")
+    region_layers = _get(bc, "regionLayers", 1, int)
+    amplitude = _get(bc, "amplitude", 0.0, float)
+    rise_time = _get(bc, "riseTime", 0.0, float)
+    plane_strain = _get(bc, "planeStrain", False, bool)
+
+    obs = _section(root, "observation")
+    axial_min = _get(obs, "axialMin", math.nan, float)
+    axial_max = _get(obs, "axialMax", math.nan, float)
+
+    dyn = _section(root, "dynamics")
+    density = _get(dyn, "density", 0.0, float)
+
+    dmg = _section(root, "damage")
+    model = _get(dmg, "model", "", str)
+    if model in ("critical_stretch", "Critical Stretch"):
+        damage_mode = DAMAGE_CRITICAL_STRETCH
+    elif model in ("", "none"):
+        damage_mode = DAMAGE_NONE
+    else:
+        raise ValueError(f"damage.model {model!r}: none or critical_stretch")
+    initiation = _get(dmg, "initiation", 0.0, float)
+    if initiation <= 0.0:
+        initiation = _get(dmg, "criticalStretch", initiation, float)
+    failure = _get(dmg, "failure", 0.0, float)
+
+    out = _section(root, "output")
+    materials = root.get("materials")
+    if not isinstance(materials, list) or not materials:
+        raise ValueError("the case needs a materials array")
+    runs = []
+    for entry in materials:
+        if not isinstance(entry, dict):
+            raise ValueError("each materials entry must be a JSON object")
+        label = _get(entry, "name", None, str)
+        if label is None:
+            raise ValueError("each material needs a name")
+        rel = _get(entry, "materialConfigPath", _get(entry, "configPath", _get(entry, "material_config_path", "", str), str), str)
+        if not rel:
+            raise ValueError(f"material {label}: materialConfigPath is required")
+        for key in ("initialState", "initialStateOverrides", "internalIndicator"):
+            if key in entry:
+                raise ValueError(f"material {label}: {key} is not supported on the device")
+        if _get(entry, "kinematicsMode", "corotational", str) != "corotational":
+            raise ValueError(f"material {label}: kinematicsMode must be corotational")
+        cfg = load_material_config(os.path.join(config_root or ".", rel))
+        eqps_index = _get(entry, "equivalentPlasticStrainIndex", -1, int)
+        if not -1 <= eqps_index < cfg["nstatev"]:
+            raise ValueError(f"material {label}: equivalentPlasticStrainIndex outside nstatev")
+        case = Case(name=f"{name}/{label}", nx=nx, ny=ny, nz=nz, spacing=spacing, horizon=horizon,
+                    dt=dt, steps=steps, density=density, props=cfg["props"],
+                    bc_mode=BC_SMOOTH_DISPLACEMENT, load_axis=0 if component == "x" else 1,
+                    region_layers=region_layers, plane_strain=plane_strain, amplitude=amplitude,
+                    rise_time=rise_time, observation_min=axial_min, observation_max=axial_max,
+                    nstatev=cfg["nstatev"],
+                    reference_temperature=_get(entry, "referenceTemperature", 293.0, float),
+                    damage_mode=damage_mode, damage_initiation=initiation, damage_failure=failure)
+        runs.append(MaterialRun(label=label, case=case, elastic_e=_get(entry, "elasticE", 0.0, float),
+                                elastic_nu=_get(entry, "elasticNu", 0.0, float), eqps_index=eqps_index,
+                                source_density=cfg["density"]))
+    return BoundaryCase(
+        name=name, classification=_get(root, "classification", "verification", str),
+        scope=_get(root, "scope", "", str), steps=steps, dt=dt,
+        output_every=_get(dyn, "outputEvery", 1, int), snapshot_every=_get(dyn, "snapshotEvery", 0, int),
+        component=component, support_region=support, load_region=load,
+        energy_tolerance=_get(dyn, "energyToleranceRelative", 1.0e-3, float),
+        net_force_tolerance=_get(dyn, "netForceTolerance", 1.0e-8, float),
+        minimum_plastic_strain=_get(dyn, "minimumPlasticStrain", 0.0, float),
+        kinetic_to_internal_limit=_get(dyn, "kineticToInternalLimit", 1.0, float),
+        output_directory=_get(out, "directory", "validation_cases/output/" + name, str),
+        materials=runs)
