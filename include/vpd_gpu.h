@@ -31,6 +31,9 @@
  *   vpd_material_update      VumatPdCorrespondenceMaterial::update (:72-176) with the
  *                            Johnson-Cook VUMAT (materials/examples/JohnsonCook.f90:12-172)
  *   vpd_damage_update        PdSimpleDamage::update, critical_stretch (src/damage/PdSimpleDamage.cpp:51-96)
+ *   vpd_set_host_vumat       VumatMaterialAdapter (src/material/VumatMaterialAdapter.cpp:238-362)
+ *                            driving any user VUMAT plugin on 256-row blocks, with the rest
+ *                            of the increment on the GPU
  *   vumat_adapter_call       the plugin entry the reference dlopens
  *                            (materials/bridge/vumat_c_wrapper_jinfo.f90:1-17,
  *                             include/VumatMaterialAdapter.hpp:35-39), Johnson-Cook on the GPU
@@ -320,6 +323,24 @@ enum { VPD_GUESS_NETWORK = 0, VPD_GUESS_WARM_START = 1, VPD_GUESS_HYBRID = 2 };
    the first vpd_step of such a handle. */
 int vpd_set_surrogate(vpd_handle *h, const uint16_t *weights, const float *biases, int32_t guess,
                       int32_t newton_steps);
+
+/* Runs the handle's material update through a host VUMAT plugin (any library exporting the
+   reference's vumat_adapter_call ABI, include/VumatMaterialAdapter.hpp:35-39, found by dlopen
+   and dlsym) in place of the device Johnson-Cook update. Each increment the GPU forms every
+   point's kinematics and packs the plugin's arguments as the reference's adapter does
+   (VumatMaterialAdapter.cpp:238-362: 256-row column-major blocks, legacy_vumat_pd order, a
+   short last block padded with its last point; step and total time at the increment's start,
+   charLength = spacing, coordinates and fields zero); the blocks are copied to pinned host
+   memory, the plugin runs on them (blocks in parallel over OpenMP threads, so it must be
+   reentrant, as the reference requires), and the stress, state, temperature and energies are
+   copied back for the force map and the diagnostics. All of it is ordered on the handle's
+   stream. cmname (blank-padded to 80), props [nprops] and density (kg/m^3, for the plugin's
+   energy terms) are the material config's; nstatev, at most the case's, is the plugin's
+   number of state variables (the case's extra ones are kept). The case's material_mode must
+   be VPD_MATERIAL_VUMAT. Call before the first vpd_step; temperatures start at the case's
+   reference_temperature. */
+int vpd_set_host_vumat(vpd_handle *h, const char *plugin_path, const char *symbol, const char *cmname,
+                       const double *props, int32_t nprops, int32_t nstatev, double density);
 
 /* Plugin ABI: the Johnson-Cook VUMAT evaluated on the GPU for one block of host arrays
    in the reference's column-major [component][nblock] layout. Synchronous. A failure is

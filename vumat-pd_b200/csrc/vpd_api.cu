@@ -495,6 +495,7 @@ void destroy_impl(vpd_handle *h) {
     cudaGraphExecDestroy(h->graph);
   if (h->stream)
     cudaStreamSynchronize(h->stream);
+  host_vumat_detach(h->params);
   for (void *p : h->allocations)
     cudaFree(p);
   free_stencil(h->st);
@@ -681,6 +682,29 @@ int vpd_set_surrogate(vpd_handle *h, const uint16_t *weights, const float *biase
   return VPD_OK;
 }
 
+int vpd_set_host_vumat(vpd_handle *h, const char *plugin_path, const char *symbol, const char *cmname,
+                       const double *props, int32_t nprops, int32_t nstatev, double density) {
+  if (!h)
+    return set_error(VPD_ERR_INVALID, "vpd_set_host_vumat: null handle");
+  if (h->c.material_mode != VPD_MATERIAL_VUMAT)
+    return set_error(VPD_ERR_INVALID, "vpd_set_host_vumat: the case's material_mode is not VPD_MATERIAL_VUMAT");
+  if (h->params.host_vumat)
+    return set_error(VPD_ERR_INVALID, "vpd_set_host_vumat: a plugin is already attached to this handle");
+  if (h->step != 0)
+    return set_error(VPD_ERR_INVALID, "vpd_set_host_vumat: call before the first vpd_step");
+  if (nstatev > h->c.nstatev)
+    return set_error(VPD_ERR_INVALID, "vpd_set_host_vumat: nstatev exceeds the case's nstatev");
+  if (!std::isfinite(density))
+    return set_error(VPD_ERR_INVALID, "vpd_set_host_vumat: density must be finite");
+  if (h->graph) {  // recaptured with the plugin's launches at the next vpd_step
+    VPD_CUDA(cudaStreamSynchronize(h->stream));
+    cudaGraphExecDestroy(h->graph);
+    h->graph = nullptr;
+  }
+  return host_vumat_attach(h->params, plugin_path, symbol, cmname, props, nprops, nstatev, density, h->c.spacing,
+                           h->c.reference_temperature, h->stream);
+}
+
 int vpd_profile_increment(vpd_handle *h, int32_t nsteps, double *stage_ms) {
   if (!h || !stage_ms || nsteps < 1)
     return set_error(VPD_ERR_INVALID, "vpd_profile_increment needs a handle, nsteps >= 1 and an output");
@@ -805,6 +829,11 @@ int vpd_download(vpd_handle *h, int32_t field, double *out) {
     return VPD_OK;
   }
   case VPD_FIELD_TEMPERATURE: {
+    if (h->params.host_vumat) {  // the plugin's tempNew, kept per point
+      VPD_CUDA(cudaMemcpyAsync(out, h->params.temp, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+      VPD_CUDA(cudaStreamSynchronize(s));
+      return VPD_OK;
+    }
     std::vector<double> st;
     int rc = getSoA(h->state, 3, st);
     if (rc)

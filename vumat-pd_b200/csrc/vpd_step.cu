@@ -525,6 +525,8 @@ int launch_stage(int stage, const StepParams &p, cudaStream_t s) {
       return p.tiled ? launch_deformation_tiled64(p, s) : launch_deformation_stencil(p, s);
     k_deformation<<<bond_grid(p.n), kBondThreads, 0, s>>>(p);
   } else if (stage == 1) {
+    if (p.host_vumat)
+      return launch_material_host(p, s);
     if (p.surrogate)
       return launch_material_surrogate(p, s);
     k_material<<<(unsigned)material_grid(p.n), kMaterialThreads, 0, s>>>(p);

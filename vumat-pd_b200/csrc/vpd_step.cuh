@@ -80,6 +80,11 @@ struct StepParams {
   int surr_steps;             // Newton steps allowed after the guess
   const uint16_t *sw;         // network weights (bf16 bits, VPD_MLP_WEIGHTS)
   const float *sb;            // network biases (400)
+  // host VUMAT plugin (vpd_set_host_vumat, vpd_hostvumat.cu); null: the device update
+  void *host_vumat;           // host-side context (never dereferenced on the device)
+  double *pack_in, *pack_out; // device blocks of the plugin's inputs and outputs
+  double *temp;               // temperature per point
+  double *mstash;             // per point: E_{n+1} - E_n (6), E along the axis, E finite
   int nstatev;
   // boundary and diagnostics sets
   const uint8_t *flags;
@@ -120,6 +125,13 @@ int launch_shape_stencil(const StepParams &p, cudaStream_t s);
 int launch_deformation_stencil(const StepParams &p, cudaStream_t s);
 int launch_force_stencil(const StepParams &p, cudaStream_t s);
 int launch_damage_index_stencil(const StepParams &p, double *out, cudaStream_t s);
+// material update through a host VUMAT plugin (vpd_hostvumat.cu): attach loads the plugin and
+// allocates its buffers into p (temperatures set to `temperature`); detach frees them
+int launch_material_host(const StepParams &p, cudaStream_t s);
+int host_vumat_attach(StepParams &p, const char *path, const char *symbol, const char *cmname, const double *props,
+                      int nprops, int nstatev, double density, double char_length, double temperature,
+                      cudaStream_t s);
+void host_vumat_detach(StepParams &p);
 // surrogate material update (vpd_surrogate.cu)
 int launch_material_surrogate(const StepParams &p, cudaStream_t s);
 int prepare_material_surrogate();  // kernel attributes; call before any capture

@@ -94,6 +94,8 @@ def library():
                                         ctypes.POINTER(SurrogateReport)]
     lib.vpd_set_surrogate.argtypes = [_VP, _VP, _VP, ctypes.c_int32, ctypes.c_int32]
     lib.vpd_mlp_gradients.argtypes = [_VP, _VP, _VP, _VP, ctypes.c_int64, _VP, _VP]
+    lib.vpd_set_host_vumat.argtypes = [_VP, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, _VP,
+                                       ctypes.c_int32, ctypes.c_int32, ctypes.c_double]
     _lib = lib
     return lib
 
@@ -201,6 +203,16 @@ class Simulation:
         _check(library().vpd_set_surrogate(self._h, None if w is None else w.ctypes.data_as(_VP),
                                            None if b is None else b.ctypes.data_as(_VP),
                                            GUESS[guess], newton_steps))
+
+    def set_host_vumat(self, plugin_path: str, props, nstatev: int, density: float,
+                       cmname: str = "JOHNSONCOOK", symbol: str = "vumat_adapter_call"):
+        """Runs the material update through a host VUMAT plugin (a shared library exporting the
+        reference's vumat_adapter_call ABI) instead of the device Johnson-Cook update; the
+        rest of each increment stays on the GPU. Call before the first step."""
+        pr = np.ascontiguousarray(props, dtype=np.float64)
+        _check(library().vpd_set_host_vumat(self._h, os.fsencode(plugin_path), symbol.encode(),
+                                            cmname.encode(), pr.ctypes.data_as(_VP), pr.size,
+                                            nstatev, density))
 
     def last_step_ms(self) -> float:
         out = ctypes.c_double()
