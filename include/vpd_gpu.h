@@ -30,7 +30,8 @@
  *                            (src/pd/CorotationalKinematics.cpp:61-149)
  *   vpd_material_update      VumatPdCorrespondenceMaterial::update (:72-176) with the
  *                            Johnson-Cook VUMAT (materials/examples/JohnsonCook.f90:12-172)
- *   vpd_damage_update        PdSimpleDamage::update, critical_stretch (src/damage/PdSimpleDamage.cpp:51-96)
+ *   vpd_damage_update        PdSimpleDamage::update, critical_stretch (src/damage/PdSimpleDamage.cpp:51-96);
+ *                            the point modes run inside vpd_step (SimpleDamageModel.cpp:14-50)
  *   vpd_set_host_vumat       VumatMaterialAdapter (src/material/VumatMaterialAdapter.cpp:238-362)
  *                            driving any user VUMAT plugin on 256-row blocks, with the rest
  *                            of the increment on the GPU
@@ -67,7 +68,15 @@ enum {
 };
 
 enum { VPD_BC_SMOOTH_DISPLACEMENT = 0, VPD_BC_VELOCITY_RAMP = 1 };
-enum { VPD_DAMAGE_NONE = 0, VPD_DAMAGE_CRITICAL_STRETCH = 1 };
+/* damage modes (SimpleDamageConfig::mode, include/SimpleDamageModel.hpp:9-17): bond breaking by
+   critical stretch, or one of the point modes of SimpleDamageModel::update
+   (src/damage/SimpleDamageModel.cpp:14-40), which degrade the spatial stress the force map uses */
+enum {
+  VPD_DAMAGE_NONE = 0,
+  VPD_DAMAGE_CRITICAL_STRETCH = 1,
+  VPD_DAMAGE_EQPS_THRESHOLD = 2,        /* metric: state variable 2 (index 1, the JC eqps) */
+  VPD_DAMAGE_MAX_PRINCIPAL_STRAIN = 3   /* metric: largest principal Green-Lagrange strain */
+};
 enum { VPD_PRECISION_FP64 = 0, VPD_PRECISION_MIXED = 1 };
 enum { VPD_MATERIAL_VUMAT = 0, VPD_MATERIAL_SURROGATE = 1 };
 
@@ -101,13 +110,17 @@ typedef struct vpd_case {
   double props[14];
   int32_t nstatev;         /* >= 6 */
   double reference_temperature;
-  /* damage (PdSimpleDamage, critical_stretch) */
+  /* damage (PdSimpleDamage) */
   int32_t damage_mode;     /* VPD_DAMAGE_* */
   double damage_initiation;
-  double damage_failure;   /* > 0 enables the compression threshold */
+  double damage_failure;   /* critical stretch: > 0 enables the compression threshold;
+                              point modes: damage = (metric - initiation) / (failure - initiation) */
   /* numerics */
   int32_t precision;       /* VPD_PRECISION_* */
   int32_t material_mode;   /* VPD_MATERIAL_* */
+  /* point damage modes: 1 deletes a fully damaged point (its stress no longer enters the force
+     map; SimpleDamageConfig::deletionEnabled) */
+  int32_t damage_deletion;
 } vpd_case;
 
 /* Per-step diagnostic row: the numeric columns of timeseries.csv in the reference's order

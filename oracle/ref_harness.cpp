@@ -170,9 +170,11 @@ void *vr_create(const vpd_case *c, const char *plugin_path) {
     s->bridge = std::make_unique<pd::VumatPdCorrespondenceMaterial>(mc);
     s->bridge->initialize(s->skeleton->computeDeformationGradients(s->block, s->cstate), s->mstate);
     SimpleDamageConfig dc;
-    dc.mode = c->damage_mode == VPD_DAMAGE_CRITICAL_STRETCH ? "critical_stretch" : "none";
+    static const char *const modes[] = {"none", "critical_stretch", "eqps_threshold", "max_principal_strain"};
+    dc.mode = c->damage_mode >= 0 && c->damage_mode <= VPD_DAMAGE_MAX_PRINCIPAL_STRAIN ? modes[c->damage_mode] : "?";
     dc.initiation = c->damage_initiation;
     dc.failure = c->damage_failure;
+    dc.deletionEnabled = c->damage_deletion != 0;
     s->damage = std::make_unique<pd::PdSimpleDamage>(dc);
     s->damage->initialize(s->block, s->dstate);
     s->integrator = std::make_unique<pd::ExplicitTimeIntegrator>(c->density);

@@ -654,6 +654,7 @@ typedef struct vo_sim {
   int64_t n, nbonds;
   double *nominal, *X, *V, *u, *v, *a, *kinv, *Fn, *Vn, *Rn, *En, *sig, *state, *temp, *eI, *eP;
   double *sigSpatial, *F, *force, *bondDamage, *damageIndex;
+  double *pointDamage, *sigEffective; /* point damage modes */
   int64_t *row_ptr;
   int32_t *col;
   vo_sets sets;
@@ -691,7 +692,8 @@ void vo_destroy(vo_sim *s) {
     return;
   double *arrs[] = {s->nominal, s->X, s->V, s->u, s->v, s->a, s->kinv, s->Fn, s->Vn, s->Rn,
                     s->En, s->sig, s->state, s->temp, s->eI, s->eP, s->sigSpatial, s->F,
-                    s->force, s->bondDamage, s->damageIndex, s->sets.obsWeight};
+                    s->force, s->bondDamage, s->damageIndex, s->sets.obsWeight,
+                    s->pointDamage, s->sigEffective};
   for (size_t k = 0; k < sizeof arrs / sizeof arrs[0]; ++k)
     free(arrs[k]);
   free(s->row_ptr), free(s->col), free(s->sets.flags), free(s);
@@ -715,7 +717,7 @@ vo_sim *vo_create(const vpd_case *c, const double *positions, const double *volu
   ALLOC(s->Vn, 9 * n), ALLOC(s->Rn, 9 * n), ALLOC(s->En, 9 * n), ALLOC(s->sig, 9 * n);
   ALLOC(s->state, (int64_t)c->nstatev * n), ALLOC(s->temp, n), ALLOC(s->eI, n), ALLOC(s->eP, n);
   ALLOC(s->sigSpatial, 9 * n), ALLOC(s->F, 9 * n), ALLOC(s->force, 3 * n);
-  ALLOC(s->damageIndex, n);
+  ALLOC(s->damageIndex, n), ALLOC(s->pointDamage, n), ALLOC(s->sigEffective, 9 * n);
   vo_lattice(c, s->nominal, s->X, s->V);
   if (positions)
     memcpy(s->X, positions, sizeof(double) * 3 * (size_t)n);
@@ -765,6 +767,52 @@ static int finite9(const double *x) {
   return 1;
 }
 
+/* maxPrincipalStrainSymmetric3x3 (TensorVoigtMap.cpp:35-71): the largest eigenvalue of the
+   symmetric part of a row-major 3x3 tensor, by the trigonometric solution of the cubic. */
+static double max_principal(const double *t) {
+  const double a = t[0], b = 0.5 * (t[1] + t[3]), c = 0.5 * (t[2] + t[6]);
+  const double d = t[4], e = 0.5 * (t[5] + t[7]), f = t[8];
+  const double p1 = b * b + c * c + e * e;
+  if (p1 == 0.0)
+    return fmax(fmax(a, d), f);
+  const double q = (a + d + f) / 3.0;
+  const double a11 = a - q, a22 = d - q, a33 = f - q;
+  const double p = sqrt((a11 * a11 + a22 * a22 + a33 * a33 + 2.0 * p1) / 6.0);
+  const double inv = 1.0 / p;
+  const double b11 = a11 * inv, b12 = b * inv, b13 = c * inv;
+  const double b22 = a22 * inv, b23 = e * inv, b33 = a33 * inv;
+  const double det = b11 * (b22 * b33 - b23 * b23) - b12 * (b12 * b33 - b23 * b13) +
+                     b13 * (b12 * b23 - b22 * b13);
+  const double h = det / 2.0;
+  const double r = h < -1.0 ? -1.0 : (1.0 < h ? 1.0 : h);
+  const double pi = 3.141592653589793238462643383279502884;
+  const double phi = acos(r) / 3.0;
+  const double e1 = q + 2.0 * p * cos(phi);
+  const double e3 = q + 2.0 * p * cos(phi + 2.0 * pi / 3.0);
+  const double e2 = 3.0 * q - e1 - e3;
+  return fmax(fmax(e1, e2), e3);
+}
+
+/* The point damage modes: SimpleDamageModel::update and degradeStress (SimpleDamageModel.cpp:14-50)
+   as PdSimpleDamage::update runs them (PdSimpleDamage.cpp:84-92). The damage follows the new eqps
+   (state variable 2) or the largest principal Green-Lagrange strain, never decreases, and scales
+   the spatial stress the force density uses; a deleted point (deletionEnabled, damage 1) drops
+   out of it. The diagnostics keep the undegraded stress. */
+static void point_damage(vo_sim *s) {
+  const vpd_case *c = &s->c;
+  for (int64_t i = 0; i < s->n; ++i) {
+    const double metric = c->damage_mode == VPD_DAMAGE_EQPS_THRESHOLD ? s->state[c->nstatev * i + 1]
+                                                                      : max_principal(s->En + 9 * i);
+    const double t = (metric - c->damage_initiation) / (c->damage_failure - c->damage_initiation);
+    const double clamped = t < 0.0 ? 0.0 : (1.0 < t ? 1.0 : t);
+    const double dmg = s->pointDamage[i] < clamped ? clamped : s->pointDamage[i];
+    s->pointDamage[i] = dmg;
+    const double factor = (c->damage_deletion && dmg >= 1.0) ? 0.0 : 1.0 - (dmg < 0.0 ? 0.0 : (1.0 < dmg ? 1.0 : dmg));
+    for (int k = 0; k < 9; ++k)
+      s->sigEffective[9 * i + k] = s->sigSpatial[9 * i + k] * factor;
+  }
+}
+
 /* The step loop body of runMaterial, BoundaryValueCaseRunner.cpp:207-306. diag: nsteps rows
    of VPD_DIAG_COLS doubles (may be NULL). */
 int vo_step(vo_sim *s, int32_t nsteps, double *diag) {
@@ -799,7 +847,12 @@ int vo_step(vo_sim *s, int32_t nsteps, double *diag) {
     if (c->damage_mode == VPD_DAMAGE_CRITICAL_STRETCH)
       vo_damage(n, s->X, s->u, s->V, s->row_ptr, s->col, c->damage_initiation, c->damage_failure,
                 s->bondDamage, s->damageIndex);
-    if ((status = vo_force(n, s->X, s->V, s->row_ptr, s->col, s->kinv, s->F, s->sigSpatial,
+    const double *sigForce = s->sigSpatial;
+    if (c->damage_mode >= VPD_DAMAGE_EQPS_THRESHOLD) {
+      point_damage(s);
+      sigForce = s->sigEffective;
+    }
+    if ((status = vo_force(n, s->X, s->V, s->row_ptr, s->col, s->kinv, s->F, sigForce,
                            s->bondDamage, s->force)) != VPD_OK)
       break;
     /* correctVelocity, ExplicitTimeIntegrator.cpp:36-52 */
@@ -940,6 +993,10 @@ int vo_get(vo_sim *s, int32_t field, double *out) {
   case VPD_FIELD_ENERGY_INTERNAL: memcpy(out, s->eI, b1); return VPD_OK;
   case VPD_FIELD_ENERGY_INELASTIC: memcpy(out, s->eP, b1); return VPD_OK;
   case VPD_FIELD_DAMAGE_INDEX:
+    if (s->c.damage_mode >= VPD_DAMAGE_EQPS_THRESHOLD) {
+      memcpy(out, s->pointDamage, b1);
+      return VPD_OK;
+    }
     for (int64_t i = 0; i < n; ++i) {
       double damaged = 0.0, total = 0.0;
       for (int64_t p = s->row_ptr[i]; p < s->row_ptr[i + 1]; ++p) {

@@ -10,7 +10,8 @@ import pytest
 from conftest import golden, load_golden_timeseries, max_rel
 
 import oracle as O
-from vpd.case import REFERENCE_JC_PROPS, Case, pd_coarse, tensile_bar
+from vpd.case import (DAMAGE_EQPS_THRESHOLD, DAMAGE_MAX_PRINCIPAL_STRAIN, REFERENCE_JC_PROPS, Case,
+                      pd_coarse, tensile_bar)
 
 
 def test_oracle_reproduces_archived_pd_coarse():
@@ -52,6 +53,27 @@ def test_oracle_matches_reference_library_live():
     assert np.array_equal(a.step(200), b.step(200))
     for field in ("displacement", "velocity", "stress_corotational", "state", "force_density"):
         assert np.array_equal(a.get(field), b.get(field)), field
+
+
+# the point damage modes (SimpleDamageModel.cpp:14-50): pd_coarse into plastic flow, thresholds
+# reached in the necking band, one case deleting its fully damaged points
+POINT_DAMAGE = [(DAMAGE_EQPS_THRESHOLD, 0.002, 0.03, False), (DAMAGE_EQPS_THRESHOLD, 0.001, 0.01, True),
+                (DAMAGE_MAX_PRINCIPAL_STRAIN, 0.005, 0.03, False)]
+
+
+@pytest.mark.skipif(not O.reference_available(), reason="reference library not built")
+@pytest.mark.parametrize("mode, initiation, failure, deletion", POINT_DAMAGE)
+def test_oracle_point_damage_matches_reference_library(mode, initiation, failure, deletion):
+    """The oracle's point damage against the reference's PdSimpleDamage / SimpleDamageModel,
+    2400 increments: bit for bit, rows and fields."""
+    case = pd_coarse().replace(steps=2400, damage_mode=mode, damage_initiation=initiation,
+                               damage_failure=failure, damage_deletion=deletion)
+    a, b = O.OracleSim(case), O.RefSim(case)
+    assert np.array_equal(a.step(2400), b.step(2400))
+    for field in ("displacement", "velocity", "state", "damage_index", "force_density"):
+        assert np.array_equal(a.get(field), b.get(field)), field
+    d = a.get("damage_index")
+    assert (d >= 1.0).sum() > 100 and (d == 0.0).sum() > 100
 
 
 def test_neighbor_lattice_regression():

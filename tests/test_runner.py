@@ -71,6 +71,22 @@ def test_unsupported_case_files_are_refused(tmp_path, edit, message):
     assert message in str(e.value)
 
 
+def test_point_damage_modes_load(tmp_path):
+    """The point modes and deletionEnabled pass through; failure defaults to 1 as in
+    SimpleDamageConfig (include/SimpleDamageModel.hpp:13-15)."""
+    with open(case_path("pd_coarse.json")) as f:
+        d = json.load(f)
+    d["damage"] = {"model": "eqps_threshold", "initiation": 0.002, "deletionEnabled": True}
+    p = tmp_path / "case.json"
+    p.write_text(json.dumps(d))
+    c = load_boundary_case(str(p), golden("")).materials[0].case
+    assert (c.damage_mode, c.damage_initiation, c.damage_failure, c.damage_deletion) == (2, 0.002, 1.0, True)
+    d["damage"] = {"model": "max_principal_strain", "initiation": 0.005, "failure": 0.03}
+    p.write_text(json.dumps(d))
+    c = load_boundary_case(str(p), golden("")).materials[0].case
+    assert (c.damage_mode, c.damage_failure, c.damage_deletion) == (3, 0.03, False)
+
+
 def archived_timeseries():
     with gzip.open(golden("pd_coarse_timeseries.csv.gz"), "rt") as f:
         text = f.read()

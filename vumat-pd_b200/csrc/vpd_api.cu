@@ -232,6 +232,7 @@ struct vpd_handle {
   unsigned *group_counter = nullptr;
   uint8_t *flags = nullptr;
   unsigned *status_dev = nullptr, *counter = nullptr;
+  double *pdmg = nullptr;      // point damage (point damage modes only)
   uint16_t *surr_w = nullptr;  // surrogate network (device copies)
   float *surr_b = nullptr;
   bool surrogate_ready = false;
@@ -274,12 +275,16 @@ int check_case(const vpd_case *c) {
   }
   if (c->damage_mode == VPD_DAMAGE_CRITICAL_STRETCH && !(c->damage_initiation > 0.0))
     return set_error(VPD_ERR_INVALID, "critical_stretch requires initiation > 0.");
-  if (c->damage_mode != VPD_DAMAGE_NONE && c->damage_mode != VPD_DAMAGE_CRITICAL_STRETCH)
+  if (c->damage_mode < VPD_DAMAGE_NONE || c->damage_mode > VPD_DAMAGE_MAX_PRINCIPAL_STRAIN)
     return set_error(VPD_ERR_INVALID, "unknown damage mode");
+  if (c->damage_mode >= VPD_DAMAGE_EQPS_THRESHOLD && !(c->damage_failure - c->damage_initiation > 0.0))
+    return set_error(VPD_ERR_INVALID, "SimpleDamageModel requires failure > initiation.");
   if (c->precision != VPD_PRECISION_FP64 && c->precision != VPD_PRECISION_MIXED)
     return set_error(VPD_ERR_INVALID, "unknown precision mode");
   if (c->material_mode != VPD_MATERIAL_VUMAT && c->material_mode != VPD_MATERIAL_SURROGATE)
     return set_error(VPD_ERR_INVALID, "unknown material mode");
+  if (c->material_mode == VPD_MATERIAL_SURROGATE && c->damage_mode >= VPD_DAMAGE_EQPS_THRESHOLD)
+    return set_error(VPD_ERR_UNSUPPORTED, "the point damage modes run with material_mode VPD_MATERIAL_VUMAT");
   for (int k = 0; k < 14; ++k)
     if (!std::isfinite(c->props[k]))
       return set_error(VPD_ERR_INVALID, "Johnson-Cook props must be finite");
@@ -350,6 +355,11 @@ int create_impl(vpd_handle *h, const vpd_case *c, const double *positions, const
       (rc = dalloc(h, &h->status_dev, 1)) || (rc = dalloc(h, &h->counter, 1)) ||
       (rc = dalloc(h, &h->accum, ACC_COUNT)) || (rc = dalloc(h, &h->diag, (size_t)kDiagRing * VPD_DIAG_COLS)))
     return rc;
+  if (c->damage_mode >= VPD_DAMAGE_EQPS_THRESHOLD) {
+    if ((rc = dalloc(h, &h->pdmg, n)))
+      return rc;
+    VPD_CUDA(cudaMemsetAsync(h->pdmg, 0, sizeof(double) * n, s));
+  }
   VPD_CUDA(cudaMemsetAsync(h->u0, 0, sizeof(double4) * n, s));
   VPD_CUDA(cudaMemsetAsync(h->status_dev, 0, sizeof(unsigned), s));
   VPD_CUDA(cudaMemsetAsync(h->counter, 0, sizeof(unsigned), s));
@@ -450,6 +460,9 @@ int create_impl(vpd_handle *h, const vpd_case *c, const double *positions, const
   p.tension2 = (1.0 + c->damage_initiation) * (1.0 + c->damage_initiation);
   p.compression2 = c->damage_failure < 1.0 ? (1.0 - c->damage_failure) * (1.0 - c->damage_failure) : 0.0;
   p.tension2f = (float)p.tension2, p.compression2f = (float)p.compression2;
+  p.point_damage = c->damage_mode >= VPD_DAMAGE_EQPS_THRESHOLD ? c->damage_mode : 0;
+  p.dmg_deletion = c->damage_deletion != 0;
+  p.pdmg = h->pdmg;
   p.surrogate = c->material_mode == VPD_MATERIAL_SURROGATE;
   if (c->precision == VPD_PRECISION_MIXED) {
     if (!h->st.nw)
@@ -696,6 +709,8 @@ int vpd_set_host_vumat(vpd_handle *h, const char *plugin_path, const char *symbo
     return set_error(VPD_ERR_INVALID, "vpd_set_host_vumat: nstatev exceeds the case's nstatev");
   if (!std::isfinite(density))
     return set_error(VPD_ERR_INVALID, "vpd_set_host_vumat: density must be finite");
+  if (h->c.damage_mode == VPD_DAMAGE_EQPS_THRESHOLD && nstatev < 2)  // SimpleDamageModel.cpp:22-25
+    return set_error(VPD_ERR_INVALID, "eqpsStateIndex is outside the VUMAT state vector.");
   if (h->graph) {  // recaptured with the plugin's launches at the next vpd_step
     VPD_CUDA(cudaStreamSynchronize(h->stream));
     cudaGraphExecDestroy(h->graph);
@@ -843,6 +858,11 @@ int vpd_download(vpd_handle *h, int32_t field, double *out) {
     return VPD_OK;
   }
   case VPD_FIELD_DAMAGE_INDEX: {
+    if (h->pdmg) {  // point modes: the point damage (PdSimpleDamage.cpp:86-92)
+      VPD_CUDA(cudaMemcpyAsync(out, h->pdmg, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+      VPD_CUDA(cudaStreamSynchronize(s));
+      return VPD_OK;
+    }
     double *d = nullptr;
     VPD_CUDA(cudaMalloc(&d, sizeof(double) * n));
     if (h->st.nw) {

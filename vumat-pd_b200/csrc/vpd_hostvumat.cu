@@ -212,7 +212,7 @@ __global__ void __launch_bounds__(kMaterialThreads, 4) k_vumat_unpack(const __gr
     p.temp[i] = get(OUT_STATE + nsc);
     m.pt.eInternal = get(OUT_STATE + nsc + 1);
     m.pt.eInelastic = get(OUT_STATE + nsc + 2);
-    material_store(p, i, m, part, maxEqps);
+    material_store<true>(p, i, m, part, maxEqps);
   }
   material_reduce(p, part, maxEqps, blockIdx.x);
 }

@@ -114,7 +114,34 @@ __device__ __forceinline__ void material_load(const StepParams &p, int64_t i, Ma
   m.inc[5] = 0.5 * (d[1] + d[3]) * p.dt;
 }
 
-// part[PM_*] and maxEqps receive this point's diagnostic contributions.
+// The point damage modes (SimpleDamageModel::update and degradeStress, SimpleDamageModel.cpp:14-50):
+// the point's damage from this increment's metric (the new eqps, or the largest principal
+// strain of E_n+1), kept non-decreasing, and the factor its spatial stress takes before the
+// force map.
+static __device__ __noinline__ double point_damage_factor(int mode, int deletion, double initiation, double failure,
+                                                   double *pdmg, const double *En, int64_t n, int64_t i,
+                                                   double eqps) {
+  double metric = eqps;  // state variable 2 (eqpsStateIndex 1)
+  if (mode == VPD_DAMAGE_MAX_PRINCIPAL_STRAIN) {
+    double E[6];
+#pragma unroll
+    for (int c = 0; c < 6; ++c)
+      E[c] = En[c * n + i];  // E_n+1, committed by material_load
+    metric = max_principal6(E);
+  }
+  const double t = (metric - initiation) / (failure - initiation);
+  const double clamped = t < 0.0 ? 0.0 : (1.0 < t ? 1.0 : t);
+  const double prev = pdmg[i];
+  const double dmg = prev < clamped ? clamped : prev;
+  pdmg[i] = dmg;
+  if (deletion && dmg >= 1.0)
+    return 0.0;
+  return 1.0 - (dmg < 0.0 ? 0.0 : (1.0 < dmg ? 1.0 : dmg));
+}
+
+// part[PM_*] and maxEqps receive this point's diagnostic contributions. POINT_DAMAGE compiles
+// in the point damage modes (kernels without it keep their registers).
+template <bool POINT_DAMAGE = false>
 __device__ __forceinline__ void material_store(const StepParams &p, int64_t i, const MaterialPoint &m, double *part,
                                                double &maxEqps) {
   const int64_t n = p.n;
@@ -131,7 +158,22 @@ __device__ __forceinline__ void material_store(const StepParams &p, int64_t i, c
   voigt_to_full(old, oldFull);
   voigt_to_full(pt.stress, full);
   rotate_to_spatial(full, R, spatial);
-  if (!force_map(spatial, F, K, M)) {
+  bool mapped;
+  if (POINT_DAMAGE && p.point_damage) {
+    // the effective stress of the force map (PdSimpleDamage.cpp:86-92); the diagnostics below
+    // keep the undegraded stress, as the reference's runner reads rawStress
+    // (BoundaryValueCaseRunner.cpp:231-259)
+    const double factor = point_damage_factor(p.point_damage, p.dmg_deletion, p.dmg_initiation, p.dmg_failure,
+                                              p.pdmg, p.En, n, i, pt.state[1]);
+    double effective[9];
+#pragma unroll
+    for (int c = 0; c < 9; ++c)
+      effective[c] = spatial[c] * factor;
+    mapped = force_map(effective, F, K, M);
+  } else {
+    mapped = force_map(spatial, F, K, M);
+  }
+  if (!mapped) {
     atomicOr(p.status, STATUS_SINGULAR_F);
 #pragma unroll
     for (int c = 0; c < 9; ++c)

@@ -87,6 +87,37 @@ __device__ __forceinline__ void green_lagrange6(const double *f, double *e6) {
   e6[5] = 0.5 * c[1];
 }
 
+// Largest eigenvalue of a symmetric tensor given in legacy Voigt order (11,22,33,23,13,12):
+// the trigonometric solution of the characteristic cubic, in the reference's order of
+// operations with every rounding spelled out (maxPrincipalStrainSymmetric3x3,
+// TensorVoigtMap.cpp:35-71). Only acos and cos may differ from the host's by an ulp.
+__device__ inline double max_principal6(const double *v) {
+  const double a = v[0], b = v[5], c = v[4], d = v[1], e = v[3], f = v[2];
+  const double p1 = __dadd_rn(__dadd_rn(__dmul_rn(b, b), __dmul_rn(c, c)), __dmul_rn(e, e));
+  if (p1 == 0.0)
+    return fmax(fmax(a, d), f);
+  const double q = __dadd_rn(__dadd_rn(a, d), f) / 3.0;
+  const double a11 = a - q, a22 = d - q, a33 = f - q;
+  const double p2 = __dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn(a11, a11), __dmul_rn(a22, a22)), __dmul_rn(a33, a33)),
+                              2.0 * p1);
+  const double pp = sqrt(p2 / 6.0);
+  const double invP = 1.0 / pp;
+  const double b11 = a11 * invP, b12 = b * invP, b13 = c * invP;
+  const double b22 = a22 * invP, b23 = e * invP, b33 = a33 * invP;
+  const double m1 = __dsub_rn(__dmul_rn(b22, b33), __dmul_rn(b23, b23));
+  const double m2 = __dsub_rn(__dmul_rn(b12, b33), __dmul_rn(b23, b13));
+  const double m3 = __dsub_rn(__dmul_rn(b12, b23), __dmul_rn(b22, b13));
+  const double detB = __dadd_rn(__dsub_rn(__dmul_rn(b11, m1), __dmul_rn(b12, m2)), __dmul_rn(b13, m3));
+  const double half = detB / 2.0;
+  const double r = half < -1.0 ? -1.0 : (1.0 < half ? 1.0 : half);
+  const double pi = 3.141592653589793238462643383279502884;
+  const double phi = acos(r) / 3.0;
+  const double eig1 = __dadd_rn(q, __dmul_rn(2.0 * pp, cos(phi)));
+  const double eig3 = __dadd_rn(q, __dmul_rn(2.0 * pp, cos(phi + 2.0 * pi / 3.0)));
+  const double eig2 = __dsub_rn(__dsub_rn(__dmul_rn(3.0, q), eig1), eig3);
+  return fmax(fmax(eig1, eig2), eig3);
+}
+
 // Symmetric tensor <-> legacy Voigt 11,22,33,23,13,12 (TensorVoigtMap.cpp:9-20).
 __device__ __forceinline__ void voigt_to_full(const double *v, double *f) {
   f[0] = v[0], f[1] = v[5], f[2] = v[4];

@@ -179,6 +179,8 @@ __global__ void __launch_bounds__(kBondThreads) k_deformation(StepParams p) {
 // Four blocks per SM (128 registers, a few hundred bytes of spills to L1): the FP64 kinematics
 // and return map are latency-bound, and the extra warps outweigh the spills (26 % faster on
 // the 250k-point bar in plastic flow than at the unconstrained 196 registers).
+// POINT_DAMAGE: the point damage modes (a separate instance, so the plain one keeps its registers).
+template <bool POINT_DAMAGE>
 __global__ void __launch_bounds__(kMaterialThreads, 4) k_material(const __grid_constant__ StepParams p) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   double part[PM_COUNT] = {};
@@ -187,7 +189,7 @@ __global__ void __launch_bounds__(kMaterialThreads, 4) k_material(const __grid_c
     MaterialPoint m;
     material_load(p, i, m);
     jc_update(p.jc, p.dt, m.inc, m.pt);
-    material_store(p, i, m, part, maxEqps);
+    material_store<POINT_DAMAGE>(p, i, m, part, maxEqps);
   }
   material_reduce(p, part, maxEqps, blockIdx.x);
 }
@@ -529,7 +531,10 @@ int launch_stage(int stage, const StepParams &p, cudaStream_t s) {
       return launch_material_host(p, s);
     if (p.surrogate)
       return launch_material_surrogate(p, s);
-    k_material<<<(unsigned)material_grid(p.n), kMaterialThreads, 0, s>>>(p);
+    if (p.point_damage)
+      k_material<true><<<(unsigned)material_grid(p.n), kMaterialThreads, 0, s>>>(p);
+    else
+      k_material<false><<<(unsigned)material_grid(p.n), kMaterialThreads, 0, s>>>(p);
   } else if (stage == 2) {
     if (p.mixed)
       return p.tiled ? launch_force_tiled(p, s) : launch_force_mixed(p, s);

@@ -94,6 +94,10 @@ struct StepParams {
   int damage;
   double dmg_initiation, dmg_failure, tension2, compression2;
   int use_compression;
+  // point damage (SimpleDamageModel::update): VPD_DAMAGE_EQPS_THRESHOLD or
+  // VPD_DAMAGE_MAX_PRINCIPAL_STRAIN, 0 otherwise
+  int point_damage, dmg_deletion;
+  double *pdmg;               // damage per point, non-decreasing
   // device bookkeeping
   int64_t *step;              // increment being computed (1-based)
   unsigned int *status;

@@ -14,7 +14,8 @@ naming the field:
   * the Johnson-Cook material (cmname JOHNSONCOOK, 14 props, 6 state variables), corotational
     stress frame, the legacy_vumat_pd tensor convention, no initial-state overrides or internal
     indicator;
-  * damage ``none`` or ``critical_stretch``.
+  * damage ``none``, ``critical_stretch`` or the point modes ``eqps_threshold`` and
+    ``max_principal_strain`` (with ``deletionEnabled``).
 """
 from __future__ import annotations
 
@@ -23,7 +24,8 @@ import json
 import math
 import os
 
-from .case import (BC_SMOOTH_DISPLACEMENT, DAMAGE_CRITICAL_STRETCH, DAMAGE_NONE, Case)
+from .case import (BC_SMOOTH_DISPLACEMENT, DAMAGE_CRITICAL_STRETCH, DAMAGE_EQPS_THRESHOLD,
+                   DAMAGE_MAX_PRINCIPAL_STRAIN, DAMAGE_NONE, Case)
 
 
 @dataclasses.dataclass
@@ -166,16 +168,18 @@ def load_boundary_case(path: str, config_root: str = None) -> BoundaryCase:
 
     dmg = _section(root, "damage")
     model = _get(dmg, "model", "", str)
-    if model in ("critical_stretch", "Critical Stretch"):
-        damage_mode = DAMAGE_CRITICAL_STRETCH
-    elif model in ("", "none"):
-        damage_mode = DAMAGE_NONE
-    else:
-        raise ValueError(f"damage.model {model!r}: none or critical_stretch")
+    modes = {"": DAMAGE_NONE, "none": DAMAGE_NONE, "critical_stretch": DAMAGE_CRITICAL_STRETCH,
+             "Critical Stretch": DAMAGE_CRITICAL_STRETCH, "eqps_threshold": DAMAGE_EQPS_THRESHOLD,
+             "max_principal_strain": DAMAGE_MAX_PRINCIPAL_STRAIN}
+    if model not in modes:
+        raise ValueError(f"damage.model {model!r}: none, critical_stretch, eqps_threshold or "
+                         "max_principal_strain")
+    damage_mode = modes[model]
     initiation = _get(dmg, "initiation", 0.0, float)
     if initiation <= 0.0:
         initiation = _get(dmg, "criticalStretch", initiation, float)
-    failure = _get(dmg, "failure", 0.0, float)
+    failure = _get(dmg, "failure", 1.0, float)  # SimpleDamageConfig's default
+    deletion = _get(dmg, "deletionEnabled", False, bool)
 
     out = _section(root, "output")
     materials = root.get("materials")
@@ -207,7 +211,8 @@ def load_boundary_case(path: str, config_root: str = None) -> BoundaryCase:
                     rise_time=rise_time, observation_min=axial_min, observation_max=axial_max,
                     nstatev=cfg["nstatev"],
                     reference_temperature=_get(entry, "referenceTemperature", 293.0, float),
-                    damage_mode=damage_mode, damage_initiation=initiation, damage_failure=failure)
+                    damage_mode=damage_mode, damage_initiation=initiation, damage_failure=failure,
+                    damage_deletion=deletion)
         runs.append(MaterialRun(label=label, case=case, elastic_e=_get(entry, "elasticE", 0.0, float),
                                 elastic_nu=_get(entry, "elasticNu", 0.0, float), eqps_index=eqps_index,
                                 source_density=cfg["density"]))

@@ -21,6 +21,8 @@ BC_SMOOTH_DISPLACEMENT = 0
 BC_VELOCITY_RAMP = 1
 DAMAGE_NONE = 0
 DAMAGE_CRITICAL_STRETCH = 1
+DAMAGE_EQPS_THRESHOLD = 2
+DAMAGE_MAX_PRINCIPAL_STRAIN = 3
 PRECISION_FP64 = 0
 PRECISION_MIXED = 1
 MATERIAL_VUMAT = 0
@@ -63,6 +65,7 @@ class VpdCase(ctypes.Structure):
         ("damage_mode", ctypes.c_int32), ("damage_initiation", ctypes.c_double),
         ("damage_failure", ctypes.c_double),
         ("precision", ctypes.c_int32), ("material_mode", ctypes.c_int32),
+        ("damage_deletion", ctypes.c_int32),
     ]
 
 
@@ -98,6 +101,7 @@ class Case:
     damage_failure: float = 0.0
     precision: int = PRECISION_FP64
     material_mode: int = MATERIAL_VUMAT
+    damage_deletion: bool = False
 
     @property
     def n_points(self) -> int:
