@@ -24,7 +24,14 @@ Fixtures (read by the tests; nothing at test time reads the reference checkout):
   pd_coarse_snapshot_head.csv.gz  the header and first 200 rows of the archived
                                raw/pd_coarse/field_snapshots.csv.gz (its text, for the writer)
 
-`--cases-only` refreshes only the last two.
+  examples/*.json, configs/elastic.json  the reference's example cases (examples/*.json,
+                               copied) and the second material config they name
+  example_outputs/<case>/*.gz  the reference's own CLI (oracle/_ref/vumat_pd_run, built from its
+                               sources by oracle/Makefile, plugins the restated JC and elastic
+                               routines) run on each example case: its output files, gzipped
+
+`--cases-only` refreshes only cases/, configs/ and the snapshot head; `--examples` only the
+example cases and their outputs.
 """
 import csv
 import gzip
@@ -55,6 +62,38 @@ def copy_cases(reference):
         head = [next(f) for _ in range(201)]
     with gzip.GzipFile(os.path.join(HERE, "pd_coarse_snapshot_head.csv.gz"), "wb", mtime=0) as g:
         g.write("".join(head).encode())
+
+
+def run_examples(reference):
+    """Copies the example cases and runs the reference's CLI on each, in a scratch directory
+    that is removed afterwards; the outputs are stored gzipped."""
+    import subprocess
+    import tempfile
+    src = os.path.join(reference, "examples")
+    names = sorted(n for n in os.listdir(src) if n.endswith(".json"))
+    os.makedirs(os.path.join(HERE, "examples"), exist_ok=True)
+    for name in names:
+        shutil.copyfile(os.path.join(src, name), os.path.join(HERE, "examples", name))
+    shutil.copyfile(os.path.join(reference, "configs", "elastic.json"),
+                    os.path.join(HERE, "configs", "elastic.json"))
+    exe = os.path.join(ROOT, "oracle", "_ref", "vumat_pd_run")
+    scratch = tempfile.mkdtemp(dir=HERE, prefix=".examples_")
+    try:
+        shutil.copytree(os.path.join(HERE, "examples"), os.path.join(scratch, "examples"))
+        shutil.copytree(os.path.join(HERE, "configs"), os.path.join(scratch, "configs"))
+        for name in names:
+            subprocess.run([exe, os.path.join("examples", name)], cwd=scratch, check=True,
+                           stdout=subprocess.DEVNULL)
+            case = name[:-5]
+            out = os.path.join(scratch, "examples", "output", case)
+            dst = os.path.join(HERE, "example_outputs", case)
+            os.makedirs(dst, exist_ok=True)
+            for f in sorted(os.listdir(out)):
+                with open(os.path.join(out, f), "rb") as a, \
+                        gzip.GzipFile(os.path.join(dst, f + ".gz"), "wb", mtime=0) as g:
+                    g.write(a.read())
+    finally:
+        shutil.rmtree(scratch)
 
 
 def main(reference):
@@ -125,5 +164,8 @@ if __name__ == "__main__":
     ref = args[0] if args else "/root/reference"
     if "--cases-only" in sys.argv:
         copy_cases(ref)
+    elif "--examples" in sys.argv:
+        run_examples(ref)
     else:
         main(ref)
+        run_examples(ref)

@@ -1,0 +1,109 @@
+"""The material-point case host (vpd.point_runner) on CPU, against the reference's own CLI.
+
+The reference's vumat_pd_run (oracle/_ref, built from its sources) and this runner both load the
+same plugin library (the restated Johnson-Cook or elastic routine in oracle/_ref) and run the
+same case file, so their output files must agree byte for byte: that pins the host logic (the
+loading path, the plane-strain bisection, the adapter's argument packing, the writers). The
+stock path, with the Johnson-Cook routine on the GPU, is checked in test_gpu_point_runner.py."""
+import gzip
+import json
+import os
+import shutil
+import subprocess
+
+import pytest
+
+from conftest import golden
+
+import oracle as O
+from vpd.point_runner import load_point_case, run_material_point_case
+
+CLI = os.path.join(O.REF_DIR, "vumat_pd_run")
+needs_cli = pytest.mark.skipif(not os.path.exists(CLI), reason="reference CLI not built")
+
+
+def fixture(case, name):
+    with gzip.open(golden(os.path.join("example_outputs", case, name + ".gz")), "rb") as f:
+        return f.read()
+
+
+def test_jc_material_point_reproduces_reference_output(tmp_path):
+    """examples/jc_material_point.json (plane strain, uniaxial stress by bisection, 600 steps)
+    against the reference CLI's files stored in tests/golden/example_outputs."""
+    rc = run_material_point_case(golden("examples/jc_material_point.json"), str(tmp_path),
+                                 config_root=golden(""), plugin_dir=O.REF_DIR, log=lambda *a: None)
+    assert rc == 0
+    for name in ("timeseries.csv", "metadata.json"):
+        assert (tmp_path / name).read_bytes() == fixture("jc_material_point", name), name
+
+
+def reference_cli(tmp_path, case):
+    """Runs the reference CLI on a case dict; returns its output directory."""
+    work = tmp_path / "ref"
+    shutil.copytree(golden("configs"), work / "configs")
+    (work / "examples").mkdir()
+    case = dict(case, output={"directory": "out"})
+    (work / "examples" / "case.json").write_text(json.dumps(case))
+    subprocess.run([CLI, "examples/case.json"], cwd=work, check=True, stdout=subprocess.DEVNULL)
+    return work / "out", work / "examples" / "case.json"
+
+
+@needs_cli
+@pytest.mark.parametrize("mode, config, reference", [
+    ("uniaxial_xx", "configs/elastic.json", True),
+    ("simple_shear_xy", "configs/elastic.json", True),
+    ("simple_shear_xy", "configs/johnson_cook.json", False),
+    ("uniaxial_xx", "configs/johnson_cook.json", False),
+])
+def test_point_modes_match_reference_cli(tmp_path, mode, config, reference):
+    with open(golden("examples/jc_material_point.json")) as f:
+        case = json.load(f)
+    case["boundary_conditions"] = {"type": "affine_displacement", "mode": mode, "maxStrain": 0.03}
+    case["time_integration"].update(steps=120, totalTime=120 * case["time_integration"]["dt"])
+    case["materials"][0].update(materialConfigPath=config, reference=reference)
+    if "elastic" in config:  # one state variable
+        case["materials"][0].update(equivalentPlasticStrainIndex=0, internalIndicator={"indices": [0]})
+    case["tolerances"] = {"referenceStressAbsolute": 1e-6}
+    ref_out, path = reference_cli(tmp_path, case)
+    ours = tmp_path / "ours"
+    rc = run_material_point_case(str(path), str(ours), config_root=str(path.parent.parent),
+                                 plugin_dir=O.REF_DIR, log=lambda *a: None)
+    for name in ("timeseries.csv", "metadata.json"):
+        assert (ours / name).read_bytes() == (ref_out / name).read_bytes(), name
+    assert rc == (0 if json.loads((ours / "metadata.json").read_text())["status"] == "pass" else 2)
+
+
+def test_point_case_loading():
+    case = load_point_case(golden("examples/jc_material_point.json"), golden(""))
+    assert (case.steps, case.dt, case.mode) == (600, 0.0002, "plane_strain_x_uniaxial_stress")
+    m = case.materials[0]
+    assert m.config.cmname == "JOHNSONCOOK" and m.config.nstatev == 6 and m.config.nfieldv == 1
+    assert m.indicator_indices == [1] and m.reference_temperature == 293.0
+    assert os.path.basename(m.config.plugin_path) == "libvpd_gpu.so"  # the stock JC on the GPU
+
+
+def test_point_case_errors(tmp_path):
+    with open(golden("examples/jc_material_point.json")) as f:
+        case = json.load(f)
+    case["materials"][0].update(materialConfigPath="configs/elastic.json", equivalentPlasticStrainIndex=0,
+                                internalIndicator={"indices": [0]})
+    p = tmp_path / "case.json"
+    p.write_text(json.dumps(case))
+    with pytest.raises(ValueError, match="plugin directory"):
+        load_point_case(str(p), golden(""))
+    with pytest.raises(RuntimeError, match="Failed to load VUMAT plugin"):
+        run_material_point_case(str(p), str(tmp_path / "o"), golden(""), str(tmp_path),
+                                log=lambda *a: None)
+    case["materials"][0]["initialState"] = [0.0, 1.0]
+    p.write_text(json.dumps(case))
+    with pytest.raises(ValueError, match="initialState length"):
+        load_point_case(str(p), golden(""), O.REF_DIR)
+    case["materials"][0].pop("initialState")
+    for edit, message in ((lambda d: d["time_integration"].update(steps=599), "totalTime"),
+                          (lambda d: d["boundary_conditions"].update(mode="biaxial"), "type or mode"),
+                          (lambda d: d.update(type="vumat_pd_boundary_case"), "vumat_material_point_case")):
+        bad = json.loads(json.dumps(case))
+        edit(bad)
+        p.write_text(json.dumps(bad))
+        with pytest.raises(ValueError, match=message):
+            load_point_case(str(p), golden(""), O.REF_DIR)

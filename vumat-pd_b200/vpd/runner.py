@@ -21,6 +21,7 @@ library that ran (``plugin_file``: libvpd_gpu.so).
 from __future__ import annotations
 
 import argparse
+import json
 import math
 import os
 import sys
@@ -250,14 +251,23 @@ def run_boundary_case(path: str, out_dir: str = None, config_root: str = None, p
 
 
 def main(argv=None) -> int:
-    ap = argparse.ArgumentParser(description="Run a reference boundary-value case file on the GPU.")
-    ap.add_argument("case", help="a vumat_pd_boundary_case JSON file")
+    """The reference's vumat_pd_run for its case files (runDemoCaseFromJson,
+    DemoCaseRunner.cpp:434-470): dispatches on the case's ``type``."""
+    ap = argparse.ArgumentParser(description="Run one of the reference's case files on the GPU.")
+    ap.add_argument("case", help="a vumat_pd_boundary_case or vumat_material_point_case JSON file")
     ap.add_argument("--out", help="output directory (default: the case's output.directory)")
     ap.add_argument("--config-root", help="directory the material config paths are relative to")
+    ap.add_argument("--plugin-dir", help="directory of the materials' VUMAT plugins (default: the "
+                    "stock Johnson-Cook plugin is this package's GPU library)")
     args = ap.parse_args(argv)
     try:
+        with open(args.case) as f:
+            kind = json.load(f).get("type", "vumat_pd_demo")
+        if kind == "vumat_material_point_case":
+            from .point_runner import run_material_point_case
+            return run_material_point_case(args.case, args.out, args.config_root, args.plugin_dir)
         return run_boundary_case(args.case, args.out, args.config_root)
-    except (ValueError, OSError) as e:
+    except (ValueError, OSError, RuntimeError) as e:
         print(f"error: {e}", file=sys.stderr)
         return 1
 
