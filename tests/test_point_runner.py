@@ -107,3 +107,38 @@ def test_point_case_errors(tmp_path):
         p.write_text(json.dumps(bad))
         with pytest.raises(ValueError, match=message):
             load_point_case(str(p), golden(""), O.REF_DIR)
+
+
+# ---------------------------------------------------------------- affine demo cases
+def test_demo_case_loading():
+    from vpd.point_runner import load_affine_case
+    case = load_affine_case(golden("examples/affine_shear_elastic.json"), "vumat_pd_demo_case",
+                            golden(""), O.REF_DIR)
+    assert (case.nx, case.ny, case.nz, case.spacing, case.horizon) == (5, 3, 3, 1.0, 1.75)
+    assert (case.steps, case.mode, case.max_strain, case.damage_model) == (20, "simple_shear_xy", 1e-4, "none")
+    assert (case.deformation_gradient_tolerance, case.reference_stress_tolerance,
+            case.net_force_tolerance) == (1e-12, 0.002, 1e-7)
+    assert case.checks and case.materials[0].config.nstatev == 1 and case.materials[0].reference
+    assert os.path.basename(case.materials[0].config.plugin_path) == "elastic_vumat_plugin.so"
+
+
+def test_demo_case_errors(tmp_path):
+    from vpd.demo_runner import run_demo_case
+    with open(golden("examples/affine_bar_elastic.json")) as f:
+        case = json.load(f)
+    case["boundary_conditions"]["maxStrain"] = 0.0
+    p = tmp_path / "case.json"
+    p.write_text(json.dumps(case))
+    with pytest.raises(ValueError, match="requires maxStrain"):
+        run_demo_case(str(p), str(tmp_path / "o"), golden(""), O.REF_DIR, log=lambda *a: None)
+    with pytest.raises(ValueError, match="plugin directory"):
+        run_demo_case(golden("examples/affine_bar_elastic.json"), str(tmp_path / "o"), golden(""),
+                      log=lambda *a: None)
+
+
+def test_runner_refuses_unknown_case_types(tmp_path, capsys):
+    from vpd.runner import main
+    p = tmp_path / "case.json"
+    p.write_text(json.dumps({"name": "x", "type": "vumat_pd_demo"}))
+    assert main([str(p)]) == 1
+    assert "Unsupported case type" in capsys.readouterr().err

@@ -46,15 +46,27 @@ class PointMaterial:
 
 
 @dataclasses.dataclass
-class PointCase:
+class AffineCase:
+    """A material-point or affine demo case: the fields of DemoCaseConfig these hosts read."""
     name: str
     scope: str
+    nx: int
+    ny: int
+    nz: int
     spacing: float
+    horizon: float
     steps: int
     dt: float
     mode: str
     max_strain: float
     reference_stress_tolerance: float
+    deformation_gradient_tolerance: float
+    net_force_tolerance: float
+    damage_model: str            # SimpleDamageConfig::mode
+    damage_initiation: float
+    damage_failure: float
+    damage_deletion: bool
+    checks: list
     output_directory: str
     materials: list
 
@@ -114,14 +126,21 @@ def _load_material(entry, config_root, plugin_dir) -> PointMaterial:
                          indicator_reduction=reduction, indicator_transform=transform)
 
 
-def load_point_case(path: str, config_root: str | None = None, plugin_dir: str | None = None) -> PointCase:
-    """A ``vumat_material_point_case`` file (DemoConfig.cpp:285-331 with its defaults)."""
+def load_point_case(path: str, config_root: str | None = None, plugin_dir: str | None = None) -> AffineCase:
+    """A ``vumat_material_point_case`` file."""
+    return load_affine_case(path, "vumat_material_point_case", config_root, plugin_dir)
+
+
+def load_affine_case(path: str, kind: str, config_root: str | None = None,
+                     plugin_dir: str | None = None) -> AffineCase:
+    """A ``vumat_material_point_case`` or ``vumat_pd_demo_case`` file (loadDemoCaseConfigFromJson,
+    DemoConfig.cpp:285-354, with its defaults and checks)."""
     with open(path) as f:
         root = json.load(f)
     if root.get("schemaVersion", "1.0") != "1.0":
         raise ValueError("Unsupported VUMAT-PD case schemaVersion: " + str(root.get("schemaVersion")))
-    if root.get("type", "vumat_pd_demo") != "vumat_material_point_case":
-        raise ValueError("not a vumat_material_point_case file")
+    if root.get("type", "vumat_pd_demo") != kind:
+        raise ValueError(f"not a {kind} file")
     name = root.get("name")
     if not isinstance(name, str):
         raise ValueError("the case needs a name")
@@ -154,6 +173,13 @@ def load_point_case(path: str, config_root: str | None = None, plugin_dir: str |
         raise ValueError("Unsupported boundary_conditions type or mode.")
     tol = root.get("tolerances") if isinstance(root.get("tolerances"), dict) else {}
     out = root.get("output") if isinstance(root.get("output"), dict) else {}
+    dmg = root.get("damage") if isinstance(root.get("damage"), dict) else {}  # loadDamage, :117-134
+    model = dmg.get("model", "")
+    model = "critical_stretch" if model in ("critical_stretch", "Critical Stretch") else (model or "none")
+    initiation = float(_num(dmg, "initiation", 0.0))
+    if initiation <= 0.0:
+        initiation = float(_num(dmg, "criticalStretch", initiation))
+    checks = [c for c in root.get("checks", []) if isinstance(c, str)] if isinstance(root.get("checks"), list) else []
     materials = root.get("materials")
     if not isinstance(materials, list):
         raise ValueError("Demo case requires a materials array.")
@@ -164,11 +190,18 @@ def load_point_case(path: str, config_root: str | None = None, plugin_dir: str |
         runs.append(_load_material(entry, config_root, plugin_dir))
     if not runs:
         raise ValueError("Demo case requires at least one material.")
-    return PointCase(name=name, scope=root.get("scope", ""), spacing=float(_num(geo, "spacing", 1.0)),
-                     steps=steps, dt=dt, mode=mode, max_strain=float(max_strain),
-                     reference_stress_tolerance=float(_num(tol, "referenceStressAbsolute", 1.0e-6)),
-                     output_directory=out.get("directory", "validation_cases/output/" + name),
-                     materials=runs)
+    return AffineCase(name=name, scope=root.get("scope", ""), nx=int(_num(geo, "nx", 1)),
+                      ny=int(_num(geo, "ny", 1)), nz=int(_num(geo, "nz", 1)),
+                      spacing=float(_num(geo, "spacing", 1.0)), horizon=float(_num(geo, "horizon", 1.0)),
+                      steps=steps, dt=dt, mode=mode, max_strain=float(max_strain),
+                      reference_stress_tolerance=float(_num(tol, "referenceStressAbsolute", 1.0e-6)),
+                      deformation_gradient_tolerance=float(_num(tol, "deformationGradientAbsolute", 1.0e-12)),
+                      net_force_tolerance=float(_num(tol, "netForceAbsolute", 1.0e-7)),
+                      damage_model=model, damage_initiation=initiation,
+                      damage_failure=float(_num(dmg, "failure", 1.0)),
+                      damage_deletion=bool(dmg.get("deletionEnabled", False)), checks=checks,
+                      output_directory=out.get("directory", "validation_cases/output/" + name),
+                      materials=runs)
 
 
 def reference_stress(m: PointMaterial, load: float, mode: str) -> float:
@@ -205,7 +238,7 @@ def _finite(values) -> bool:
     return all(math.isfinite(v) for v in values)
 
 
-def run_material(case: PointCase, m: PointMaterial, lines: list) -> dict:
+def run_material(case: AffineCase, m: PointMaterial, lines: list) -> dict:
     """runMaterial (:73-183) for one material; appends its timeseries lines."""
     plugin = VumatPlugin(m.config)
     dt = case.dt
@@ -290,7 +323,7 @@ def run_material(case: PointCase, m: PointMaterial, lines: list) -> dict:
     return summary
 
 
-def metadata_text(case: PointCase, summaries: list, passed: bool) -> str:
+def metadata_text(case: AffineCase, summaries: list, passed: bool) -> str:
     """metadata.json of runMaterialPointCase (:200-222)."""
     def b(v):
         return "true" if v else "false"

@@ -1,5 +1,8 @@
-"""Runs one of the reference's JSON boundary-value cases on the GPU and writes the reference's
-output files: timeseries.csv, field_snapshots.csv and metadata.json in the layout of its case
+"""Runs one of the reference's JSON case files (``python -m vpd.runner CASE.json``), as its
+``vumat_pd_run`` does: by the case's ``type``, a boundary-value case (this module), a
+material-point case (``vpd.point_runner``) or an affine demo case (``vpd.demo_runner``).
+
+A boundary-value case runs on the GPU and writes the reference's output files: timeseries.csv, field_snapshots.csv and metadata.json in the layout of its case
 runner (runBoundaryValueCase, src/host/BoundaryValueCaseRunner.cpp:341-439), so the
 reference's analysis scripts read them unchanged.
 
@@ -254,7 +257,8 @@ def main(argv=None) -> int:
     """The reference's vumat_pd_run for its case files (runDemoCaseFromJson,
     DemoCaseRunner.cpp:434-470): dispatches on the case's ``type``."""
     ap = argparse.ArgumentParser(description="Run one of the reference's case files on the GPU.")
-    ap.add_argument("case", help="a vumat_pd_boundary_case or vumat_material_point_case JSON file")
+    ap.add_argument("case", help="a vumat_pd_boundary_case, vumat_material_point_case or "
+                    "vumat_pd_demo_case JSON file")
     ap.add_argument("--out", help="output directory (default: the case's output.directory)")
     ap.add_argument("--config-root", help="directory the material config paths are relative to")
     ap.add_argument("--plugin-dir", help="directory of the materials' VUMAT plugins (default: the "
@@ -266,6 +270,11 @@ def main(argv=None) -> int:
         if kind == "vumat_material_point_case":
             from .point_runner import run_material_point_case
             return run_material_point_case(args.case, args.out, args.config_root, args.plugin_dir)
+        if kind == "vumat_pd_demo_case":
+            from .demo_runner import run_demo_case
+            return run_demo_case(args.case, args.out, args.config_root, args.plugin_dir)
+        if kind != "vumat_pd_boundary_case":
+            raise ValueError("Unsupported case type: " + str(kind))
         return run_boundary_case(args.case, args.out, args.config_root)
     except (ValueError, OSError, RuntimeError) as e:
         print(f"error: {e}", file=sys.stderr)

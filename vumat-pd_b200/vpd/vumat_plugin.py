@@ -1,11 +1,11 @@
-"""VUMAT material configs and single-point plugin calls, for the material-point case host.
+"""VUMAT material configs and plugin calls, for the material-point and affine demo case hosts.
 
 ``load_vumat_config`` reads a material config (configs/*.json; the reference's
-src/config/MaterialConfigJson.cpp:63-101, same defaults and checks) for any VUMAT, and
-``VumatPlugin.update_point`` makes one call of the plugin's ``vumat_adapter_call`` on a single
-point, packing and unpacking its arguments as the reference's adapter does for a one-point
-block (VumatMaterialAdapter::updatePoint and updateFixedBlockCached,
-src/material/VumatMaterialAdapter.cpp:116-147 and 238-362).
+src/config/MaterialConfigJson.cpp:63-101, same defaults and checks) for any VUMAT.
+``VumatPlugin.update_block`` makes one call of the plugin's ``vumat_adapter_call`` on up to 256
+rows, packing and unpacking its arguments as the reference's adapter does
+(VumatMaterialAdapter::updateFixedBlockCached, src/material/VumatMaterialAdapter.cpp:238-362);
+``update_point`` is the one-row call of VumatMaterialAdapter::updatePoint (:116-147).
 
 Plugins are found as the reference finds them: ``pluginPath``, or ``plugin`` plus ``.so``,
 relative to the plugin directory. Without a plugin directory the stock Johnson-Cook plugin
@@ -102,16 +102,10 @@ def load_vumat_config(path: str, plugin_dir: str | None = None) -> VumatConfig:
                        props=tuple(float(p) for p in props), density=density, stress_frame=frame)
 
 
-def _voigt(t):  # fullTensorToVumatVoigt, TensorVoigtMap.cpp:9-16
-    return (t[0], t[4], t[8], 0.5 * (t[5] + t[7]), 0.5 * (t[2] + t[6]), 0.5 * (t[1] + t[3]))
-
-
-def _full(v):  # vumatVoigtToFullTensor, TensorVoigtMap.cpp:18-20
-    return [v[0], v[5], v[4], v[5], v[1], v[3], v[4], v[3], v[2]]
-
-
-def _defgrad(t):  # fullTensorToVumatDefgrad, TensorVoigtMap.cpp:22-24
-    return (t[0], t[4], t[8], t[1], t[5], t[6], t[3], t[7], t[2])
+def _voigt_rows(t):
+    """fullTensorToVumatVoigt (TensorVoigtMap.cpp:9-16) of each row of t [nb, 9] -> [6, nb]."""
+    return np.stack([t[:, 0], t[:, 4], t[:, 8], 0.5 * (t[:, 5] + t[:, 7]), 0.5 * (t[:, 2] + t[:, 6]),
+                     0.5 * (t[:, 1] + t[:, 3])])
 
 
 @dataclasses.dataclass
@@ -174,45 +168,78 @@ class VumatPlugin:
         self._props = np.array(config.props, dtype=np.float64)
         self._cmname = config.cmname.encode()[:80].ljust(80, b" ")
 
-    def update_point(self, p: PointInput) -> PointResult:
-        """One point through the plugin: updatePoint as a one-row block."""
+    def update_block(self, *, dt, step_time, total_time, char_length, temperature, strain_rate,
+                     rel_spin, stress_n, stretch_old, stretch_new, defgrad_old, defgrad_new,
+                     state_old, internal_energy_old, inelastic_energy_old) -> dict:
+        """One plugin call on nb <= 256 rows (updateFixedBlockCached, :238-362). Tensors are
+        [nb, 9] row-major full tensors, state_old [nb, nstatev], the rest [nb]. Returns the new
+        full stress [nb, 9], state [nb, nstatev], temperature and energies [nb]."""
         c = self.config
-        if not (math.isfinite(p.dt) and p.dt > 0.0):
-            raise ValueError("VUMAT update requires dt > 0.")
-        if len(p.state_old) != c.nstatev:
+        if not (math.isfinite(dt) and dt > 0.0):
+            raise ValueError("Cached material update requires a positive time step and at most 256 points.")
+        f = lambda a: np.ascontiguousarray(a, dtype=np.float64)  # noqa: E731
+        strain_rate, rel_spin, stress_n = f(strain_rate), f(rel_spin), f(stress_n)
+        stretch_old, stretch_new = f(stretch_old), f(stretch_new)
+        defgrad_old, defgrad_new, state_old = f(defgrad_old), f(defgrad_new), f(state_old)
+        nb = strain_rate.shape[0]
+        if not 1 <= nb <= 256:
+            raise ValueError("Cached material update requires a positive time step and at most 256 points.")
+        if state_old.shape != (nb, c.nstatev):
             raise ValueError("stateOld entry size does not match nstatev.")
-
-        def arr(values):
-            return np.array(values, dtype=np.float64)
-
-        field_cols, state_cols = max(1, c.nfieldv), max(1, c.nstatev)
-        stress_old = arr(_voigt(p.stress_n))
-        strain_inc = arr([v * p.dt for v in _voigt(p.strain_rate)])
-        spin = arr((p.rel_spin[5], p.rel_spin[6], p.rel_spin[1]))
-        stretch_old, stretch_new = arr(_voigt(p.stretch_old)), arr(_voigt(p.stretch_new))
-        defgrad_old, defgrad_new = arr(_defgrad(p.defgrad_old)), arr(_defgrad(p.defgrad_new))
-        state_old = np.zeros(state_cols)
-        state_old[:c.nstatev] = p.state_old
-        temp_old, temp_new = arr([p.temperature]), arr([p.temperature])
-        ei_old, ep_old = arr([p.internal_energy_old]), arr([p.inelastic_energy_old])
-        ei_new, ep_new = arr([p.internal_energy_old]), arr([p.inelastic_energy_old])
-        stress_new, state_new = np.zeros(6), np.zeros(state_cols)
-        coord, char_length, density = np.zeros(3), arr([p.char_length]), arr([c.density])
-        field_old, field_new = np.zeros(field_cols), np.zeros(field_cols)
+        # [component][nblock] column-major blocks, as the adapter's work arrays
+        strain_inc = np.ascontiguousarray(_voigt_rows(strain_rate) * dt)
+        spin = np.ascontiguousarray(np.stack([rel_spin[:, 5], rel_spin[:, 6], rel_spin[:, 1]]))
+        stress_old = np.ascontiguousarray(_voigt_rows(stress_n))
+        v_old, v_new = np.ascontiguousarray(_voigt_rows(stretch_old)), np.ascontiguousarray(_voigt_rows(stretch_new))
+        order = [0, 4, 8, 1, 5, 6, 3, 7, 2]  # fullTensorToVumatDefgrad
+        g_old = np.ascontiguousarray(defgrad_old[:, order].T)
+        g_new = np.ascontiguousarray(defgrad_new[:, order].T)
+        state_cols, field_cols = max(1, c.nstatev), max(1, c.nfieldv)
+        st_old = np.zeros((state_cols, nb))
+        st_old[:c.nstatev] = state_old.T
+        temp_old = f(temperature).copy()
+        temp_new = temp_old.copy()
+        ei_old, ep_old = f(internal_energy_old).copy(), f(inelastic_energy_old).copy()
+        ei_new, ep_new = ei_old.copy(), ep_old.copy()
+        stress_new, state_new = np.zeros((6, nb)), np.zeros((state_cols, nb))
+        coord, length = np.zeros(3 * nb), f(char_length).copy()
+        density = np.full(nb, c.density)
+        field_old, field_new = np.zeros(field_cols * nb), np.zeros(field_cols * nb)
         props = self._props.copy()
-        ints = [ctypes.c_int(v) for v in (1, 3, 3, c.nstatev, c.nfieldv, len(c.props), 0)]
-        times = [ctypes.c_double(v) for v in (p.step_time, p.total_time, p.dt)]
+        ints = [ctypes.c_int(v) for v in (nb, 3, 3, c.nstatev, c.nfieldv, len(c.props), 0)]
+        times = [ctypes.c_double(v) for v in (step_time, total_time, dt)]
 
         def dp(a):
             return a.ctypes.data_as(_DP)
 
         self._call(*[ctypes.byref(v) for v in ints], *[ctypes.byref(v) for v in times],
                    ctypes.create_string_buffer(self._cmname, 80),
-                   dp(coord), dp(char_length), dp(props), dp(density), dp(strain_inc), dp(spin),
-                   dp(temp_old), dp(stretch_old), dp(defgrad_old), dp(field_old), dp(stress_old),
-                   dp(state_old), dp(ei_old), dp(ep_old), dp(temp_new), dp(stretch_new),
-                   dp(defgrad_new), dp(field_new), dp(stress_new), dp(state_new), dp(ei_new),
-                   dp(ep_new))
-        return PointResult(stress=_full(stress_new.tolist()), state=state_new[:c.nstatev].tolist(),
-                           temperature=float(temp_new[0]), internal_energy=float(ei_new[0]),
-                           inelastic_energy=float(ep_new[0]))
+                   dp(coord), dp(length), dp(props), dp(density), dp(strain_inc), dp(spin),
+                   dp(temp_old), dp(v_old), dp(g_old), dp(field_old), dp(stress_old),
+                   dp(st_old), dp(ei_old), dp(ep_old), dp(temp_new), dp(v_new),
+                   dp(g_new), dp(field_new), dp(stress_new), dp(state_new), dp(ei_new), dp(ep_new))
+        v = stress_new  # vumatVoigtToFullTensor
+        full = np.stack([v[0], v[5], v[4], v[5], v[1], v[3], v[4], v[3], v[2]], axis=1)
+        return dict(stress=full, state=state_new[:c.nstatev].T.copy(), temperature=temp_new,
+                    internal_energy=ei_new, inelastic_energy=ep_new)
+
+    def update_point(self, p: PointInput) -> PointResult:
+        """One point through the plugin: updatePoint as a one-row block (:116-147)."""
+        if not (math.isfinite(p.dt) and p.dt > 0.0):
+            raise ValueError("VUMAT update requires dt > 0.")
+        if len(p.state_old) != self.config.nstatev:
+            raise ValueError("stateOld entry size does not match nstatev.")
+        row = lambda t: np.array([t], dtype=np.float64)  # noqa: E731
+        r = self.update_block(dt=p.dt, step_time=p.step_time, total_time=p.total_time,
+                              char_length=[p.char_length], temperature=[p.temperature],
+                              strain_rate=row(p.strain_rate), rel_spin=row(p.rel_spin),
+                              stress_n=row(p.stress_n), stretch_old=row(p.stretch_old),
+                              stretch_new=row(p.stretch_new), defgrad_old=row(p.defgrad_old),
+                              defgrad_new=row(p.defgrad_new),
+                              state_old=np.array([p.state_old], dtype=np.float64).reshape(1, -1),
+                              internal_energy_old=[p.internal_energy_old],
+                              inelastic_energy_old=[p.inelastic_energy_old])
+        return PointResult(stress=r["stress"][0].tolist(), state=r["state"][0].tolist(),
+                           temperature=float(r["temperature"][0]),
+                           internal_energy=float(r["internal_energy"][0]),
+                           inelastic_energy=float(r["inelastic_energy"][0]))
