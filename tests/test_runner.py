@@ -187,3 +187,24 @@ def test_snapshot_steps_and_observation_window():
     assert observation_bounds(x, 0, 2.0, 10.0, 90.0) == (10.0, 90.0)
     with pytest.raises(ValueError):
         observation_bounds(x, 0, 2.0, 50.0, 40.0)
+
+
+def test_boundary_case_with_a_host_plugin(tmp_path):
+    """A material config naming another plugin loads for the host plugin path: its props,
+    state count and plugin are kept for set_host_vumat, the case carries the device layout's
+    6 state columns, and eqps must be state variable 2 or none."""
+    import oracle as O
+    with open(case_path("pd_coarse.json")) as f:
+        d = json.load(f)
+    d["materials"][0].update(materialConfigPath="configs/elastic.json", equivalentPlasticStrainIndex=-1)
+    p = tmp_path / "case.json"
+    p.write_text(json.dumps(d))
+    m = load_boundary_case(str(p), golden(""), O.REF_DIR).materials[0]
+    assert m.host_plugin is not None and m.host_plugin.nstatev == 1 and m.host_plugin.props == (210000.0, 0.3)
+    assert os.path.basename(m.host_plugin.plugin_path) == "elastic_vumat_plugin.so"
+    assert m.case.nstatev == 6 and m.case.props == (0.0,) * 14 and m.eqps_index == -1
+    d["materials"][0]["equivalentPlasticStrainIndex"] = 0
+    p.write_text(json.dumps(d))
+    with pytest.raises(ValueError, match="must be 1 or -1"):
+        load_boundary_case(str(p), golden(""), O.REF_DIR)
+    assert load_boundary_case(case_path("pd_coarse.json"), golden("")).materials[0].host_plugin is None

@@ -11,9 +11,10 @@ naming the field:
   * boundary type ``regional_smooth_displacement`` (half-cosine displacement of the load band,
     BoundaryConditions.cpp:70-79), loading component x (support ``left``, load ``right``) or
     y (``bottom``/``top``), rigid-body suppression on;
-  * the Johnson-Cook material (cmname JOHNSONCOOK, 14 props, 6 state variables), corotational
-    stress frame, the legacy_vumat_pd tensor convention, no initial-state overrides or internal
-    indicator;
+  * the stock Johnson-Cook plugin as the device update, or any other VUMAT plugin through the
+    host plugin path (found in the plugin directory); the corotational stress frame, the
+    legacy_vumat_pd tensor convention, eqps at state variable 2 or none, no initial-state
+    overrides or internal indicator;
   * damage ``none``, ``critical_stretch`` or the point modes ``eqps_threshold`` and
     ``max_principal_strain`` (with ``deletionEnabled``).
 """
@@ -24,6 +25,7 @@ import json
 import math
 import os
 
+from .vumat_plugin import load_vumat_config
 from .case import (BC_SMOOTH_DISPLACEMENT, DAMAGE_CRITICAL_STRETCH, DAMAGE_EQPS_THRESHOLD,
                    DAMAGE_MAX_PRINCIPAL_STRAIN, DAMAGE_NONE, Case)
 
@@ -37,6 +39,7 @@ class MaterialRun:
     elastic_nu: float
     eqps_index: int                  # state variable written as eqps (-1: none)
     source_density: float            # the material config's density (kg/m^3)
+    host_plugin: object = None       # VumatConfig of a plugin run on the host (None: device JC)
 
 
 @dataclasses.dataclass
@@ -87,34 +90,35 @@ def _section(root, key):
     return obj
 
 
-def load_material_config(path: str) -> dict:
-    """A VUMAT material config (configs/*.json), checked against what the device VUMAT runs."""
-    with open(path) as f:
-        root = json.load(f)
-    if _get(root, "schemaVersion", "1.0", str) != "1.0":
-        raise ValueError(f"{path}: unsupported material schemaVersion")
-    cmname = _get(root, "cmname", "", str)
-    if cmname.upper() != "JOHNSONCOOK":
-        raise ValueError(f"{path}: cmname {cmname!r}: only the Johnson-Cook VUMAT runs on the device")
-    if _get(root, "tensorConvention", "legacy_vumat_pd", str) != "legacy_vumat_pd":
-        raise ValueError(f"{path}: tensorConvention must be legacy_vumat_pd")
-    if _get(root, "stressFrame", "corotational", str) != "corotational":
+def load_material_config(path: str, plugin_dir: str = None) -> dict:
+    """A VUMAT material config (configs/*.json; MaterialConfigJson.cpp:63-101). The stock
+    Johnson-Cook plugin runs as the device update; any other plugin (found as
+    ``vpd.vumat_plugin.load_vumat_config`` finds it) runs through the host plugin path
+    (``Simulation.set_host_vumat``), and its entry is returned as ``host_plugin``."""
+    from . import library_path
+    try:
+        cfg = load_vumat_config(path, plugin_dir)
+    except ValueError as e:
+        raise ValueError(f"{path}: {e}") from None
+    if cfg.stress_frame != "corotational":
         raise ValueError(f"{path}: boundary cases need the corotational stress frame")
-    if _get(root, "ndir", 3, int) != 3 or _get(root, "nshr", 3, int) != 3:
-        raise ValueError(f"{path}: ndir and nshr must be 3")
-    nstatev = _get(root, "nstatev", 0, int)
-    props = root.get("props")
-    if not isinstance(props, list) or len(props) != 14 or nstatev != 6:
-        raise ValueError(f"{path}: Johnson-Cook needs 14 props and 6 state variables")
-    density = _get(root, "density", 0.0, float)
-    if density <= 0.0:
-        raise ValueError(f"{path}: density must be positive")
-    return {"props": tuple(float(p) for p in props), "nstatev": nstatev, "density": density}
+    if cfg.plugin_path == library_path():  # the device Johnson-Cook update
+        if cfg.cmname.upper() != "JOHNSONCOOK" or len(cfg.props) != 14 or cfg.nstatev != 6:
+            raise ValueError(f"{path}: the Johnson-Cook plugin needs cmname JOHNSONCOOK, 14 props "
+                             "and 6 state variables")
+        return {"props": cfg.props, "nstatev": 6, "density": cfg.density, "host_plugin": None}
+    if not cfg.props:
+        raise ValueError(f"{path}: VUMAT props cannot be empty.")
+    # the case's own 14 props are not read with a host plugin; the state keeps at least the 6
+    # columns the device layout has
+    return {"props": (0.0,) * 14, "nstatev": max(6, cfg.nstatev), "density": cfg.density,
+            "host_plugin": cfg}
 
 
-def load_boundary_case(path: str, config_root: str = None) -> BoundaryCase:
+def load_boundary_case(path: str, config_root: str = None, plugin_dir: str = None) -> BoundaryCase:
     """Reads a boundary-value case file. Material config paths are resolved against
-    ``config_root`` (default: the current directory, as the reference's host resolves them)."""
+    ``config_root`` (default: the current directory, as the reference's host resolves them),
+    plugins other than the stock Johnson-Cook one against ``plugin_dir``."""
     with open(path) as f:
         root = json.load(f)
     if _get(root, "schemaVersion", "1.0", str) != "1.0":
@@ -200,10 +204,14 @@ def load_boundary_case(path: str, config_root: str = None) -> BoundaryCase:
                 raise ValueError(f"material {label}: {key} is not supported on the device")
         if _get(entry, "kinematicsMode", "corotational", str) != "corotational":
             raise ValueError(f"material {label}: kinematicsMode must be corotational")
-        cfg = load_material_config(os.path.join(config_root or ".", rel))
+        cfg = load_material_config(os.path.join(config_root or ".", rel), plugin_dir)
         eqps_index = _get(entry, "equivalentPlasticStrainIndex", -1, int)
-        if not -1 <= eqps_index < cfg["nstatev"]:
+        nstatev = cfg["host_plugin"].nstatev if cfg["host_plugin"] else cfg["nstatev"]
+        if not -1 <= eqps_index < nstatev:
             raise ValueError(f"material {label}: equivalentPlasticStrainIndex outside nstatev")
+        if eqps_index not in (-1, 1):
+            raise ValueError(f"material {label}: the device reduces state variable 2 as eqps; "
+                             "equivalentPlasticStrainIndex must be 1 or -1")
         case = Case(name=f"{name}/{label}", nx=nx, ny=ny, nz=nz, spacing=spacing, horizon=horizon,
                     dt=dt, steps=steps, density=density, props=cfg["props"],
                     bc_mode=BC_SMOOTH_DISPLACEMENT, load_axis=0 if component == "x" else 1,
@@ -215,7 +223,7 @@ def load_boundary_case(path: str, config_root: str = None) -> BoundaryCase:
                     damage_deletion=deletion)
         runs.append(MaterialRun(label=label, case=case, elastic_e=_get(entry, "elasticE", 0.0, float),
                                 elastic_nu=_get(entry, "elasticNu", 0.0, float), eqps_index=eqps_index,
-                                source_density=cfg["density"]))
+                                source_density=cfg["density"], host_plugin=cfg["host_plugin"]))
     return BoundaryCase(
         name=name, classification=_get(root, "classification", "verification", str),
         scope=_get(root, "scope", "", str), steps=steps, dt=dt,

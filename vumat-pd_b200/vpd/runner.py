@@ -163,7 +163,7 @@ def metadata_text(bc: BoundaryCase, summaries: list) -> str:
     for m, s in zip(bc.materials, summaries):
         items.append(
             f"    {{\"name\": \"{m.label}\", \"status\": \"{'pass' if s['pass'] else 'fail'}\", "
-            f"\"plugin_file\": \"libvpd_gpu.so\", \"sourceDensity_kg_per_m3\": {json_number(m.source_density)}, "
+            f"\"plugin_file\": \"{plugin_file(m)}\", \"sourceDensity_kg_per_m3\": {json_number(m.source_density)}, "
             f"\"solverDensity\": {json_number(m.case.density)}, \"runtimeSeconds\": {json_number(s['runtimeSeconds'])}, "
             f"\"observationAxis\": \"{bc.component}\", \"observationMin_mm\": {json_number(s['observationMin'])}, "
             f"\"observationMax_mm\": {json_number(s['observationMax'])}, "
@@ -202,13 +202,18 @@ def snapshot_steps(bc: BoundaryCase) -> list:
     return sorted(marks)
 
 
+def plugin_file(m) -> str:
+    """The metadata's plugin_file: the library whose material routine ran."""
+    return os.path.basename(m.host_plugin.plugin_path) if m.host_plugin is not None else "libvpd_gpu.so"
+
+
 def run_boundary_case(path: str, out_dir: str = None, config_root: str = None, precision: int = None,
-                      log=print) -> int:
+                      log=print, plugin_dir: str = None) -> int:
     """Runs every material of a boundary-value case file and writes its three output files into
     ``out_dir`` (default: the case's output.directory). Returns 0 when every material passes
     the case's acceptance limits, 2 otherwise (the reference runner's exit status)."""
     from . import Simulation
-    bc = load_boundary_case(path, config_root)
+    bc = load_boundary_case(path, config_root, plugin_dir)
     out = out_dir or bc.output_directory
     os.makedirs(out, exist_ok=True)
     summaries = []
@@ -222,6 +227,10 @@ def run_boundary_case(path: str, out_dir: str = None, config_root: str = None, p
             started = time.perf_counter()
             chunks, done = [], 0
             with Simulation(case) as sim:
+                if m.host_plugin is not None:
+                    p = m.host_plugin
+                    sim.set_host_vumat(p.plugin_path, p.props, p.nstatev, p.density, cmname=p.cmname,
+                                       symbol=p.symbol)
                 x0 = sim.field("position")
                 lo, hi = observation_bounds(x0, axis, (case.region_layers - 1) * case.spacing,
                                             case.observation_min, case.observation_max)
@@ -237,6 +246,8 @@ def run_boundary_case(path: str, out_dir: str = None, config_root: str = None, p
                                             sim.field("damage_index")[:, 0]))
             runtime = time.perf_counter() - started
             rows = np.concatenate(chunks)
+            if m.eqps_index < 0:  # no eqps variable: the reference reports 0 (:259-261)
+                rows[:, DIAG["max_eqps"]] = 0.0
             for row in rows:
                 step = int(row[DIAG["step"]])
                 if step % bc.output_every == 0 or step == 1 or step == bc.steps:
@@ -275,7 +286,7 @@ def main(argv=None) -> int:
             return run_demo_case(args.case, args.out, args.config_root, args.plugin_dir)
         if kind != "vumat_pd_boundary_case":
             raise ValueError("Unsupported case type: " + str(kind))
-        return run_boundary_case(args.case, args.out, args.config_root)
+        return run_boundary_case(args.case, args.out, args.config_root, plugin_dir=args.plugin_dir)
     except (ValueError, OSError, RuntimeError) as e:
         print(f"error: {e}", file=sys.stderr)
         return 1
