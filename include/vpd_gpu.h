@@ -208,6 +208,21 @@ int vpd_last_step_ms(const vpd_handle *h, double *ms);
    device only.
    (No reference counterpart: per-stage timing of the step loop.) */
 int vpd_profile_increment(vpd_handle *h, int32_t nsteps, double *stage_ms);
+/* Checkpoint and resume between increments. A checkpoint holds the state one increment
+   carries to the next: displacements, velocities, accelerations and forces; the material
+   history (F, V, R, E, stress, state, energies); broken bonds; point damage and plugin
+   temperatures where used; the running energy sums and the increment count. It does not
+   hold what the case and the attached material determine (geometry, bonds, K^-1, the sets,
+   the network). vpd_checkpoint_bytes gives the size; vpd_checkpoint_save fills a host buffer
+   of exactly that size. vpd_checkpoint_load restores one into a handle created from the same
+   case (and, before the load, given the same vpd_set_surrogate or vpd_set_host_vumat), which
+   then continues bit for bit as the saved handle would have; a checkpoint of another case,
+   layout, precision or material path is refused. The diagnostic rows of later vpd_step calls
+   continue the saved run's step numbers.
+   (No reference counterpart: the reference keeps no state between runs.) */
+int64_t vpd_checkpoint_bytes(vpd_handle *h);
+int vpd_checkpoint_save(vpd_handle *h, void *buffer, int64_t bytes);
+int vpd_checkpoint_load(vpd_handle *h, const void *buffer, int64_t bytes);
 
 /* ---- module-level entry points (device pointers, caller-owned) ---- */
 

@@ -12,6 +12,12 @@ sys.path.insert(0, os.path.join(ROOT, "vumat-pd_b200"))
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200) and libvpd_gpu.so")
+    config.addinivalue_line("markers", "late: runs after the other tests, so that a failure under -x "
+                                       "leaves their results in place (tests not yet run on a GPU)")
+
+
+def pytest_collection_modifyitems(session, config, items):
+    items.sort(key=lambda item: item.get_closest_marker("late") is not None)  # stable
 
 
 def golden(name):

@@ -22,7 +22,7 @@ from conftest import golden
 import oracle as O
 from vpd.runner import run_boundary_case
 
-pytestmark = pytest.mark.gpu
+pytestmark = [pytest.mark.gpu, pytest.mark.late]
 CLI = os.path.join(O.REF_DIR, "vumat_pd_run")
 
 

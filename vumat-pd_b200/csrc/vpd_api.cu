@@ -562,6 +562,75 @@ template <typename Fn> int with_host_buffer(size_t count, Fn &&fn) {
   return fn(buf);
 }
 
+// ---- checkpoint / resume ----
+// The state an increment carries to the next, as (device pointer, bytes) sections in a fixed
+// order: everything else is either fixed at creation (geometry, bonds, K^-1, the sets) or
+// recomputed inside every increment (F, the force map, the mixed-precision sums, the
+// diagnostic partials and counters).
+struct Section {
+  void *ptr;
+  size_t bytes;
+};
+
+std::vector<Section> checkpoint_sections(vpd_handle *h) {
+  const size_t n = (size_t)h->n, d4 = sizeof(double4) * n, d1 = sizeof(double) * n;
+  const StepParams &p = h->params;
+  std::vector<Section> v = {{h->u0, d4}, {h->u1, d4},     {h->vel, d4},     {h->acc, d4},
+                            {h->force, d4}, {h->Fn, 9 * d1}, {h->Vn, 9 * d1}, {h->Rn, 9 * d1},
+                            {h->En, 6 * d1}, {h->sig, 6 * d1}, {h->state, (size_t)h->c.nstatev * d1},
+                            {h->eI, d1},     {h->eP, d1},     {h->accum, sizeof(double) * ACC_COUNT},
+                            {h->step_dev, sizeof(int64_t)}};
+  if (h->words)
+    v.push_back({h->words, sizeof(uint32_t) * (size_t)(h->sell_total / 32)});
+  if (h->st.nw)
+    v.push_back({h->st.broken, sizeof(uint32_t) * (size_t)h->st.nw * n});
+  if (p.mixed)
+    v.push_back({p.uf, sizeof(float4) * n});
+  if (h->pdmg)
+    v.push_back({h->pdmg, d1});
+  if (p.host_vumat)
+    v.push_back({p.temp, d1});
+  return v;
+}
+
+// What the loading handle must share with the saving one.
+struct CheckpointHeader {
+  char magic[8];
+  uint32_t version, sections;
+  int64_t step, n, nbonds, sell_total;
+  int32_t stencil_words, mixed, host_vumat, surrogate;
+  uint64_t payload;
+  vpd_case c;
+};
+
+// Field by field, bitwise (NaN observation bounds compare equal); padding is not compared.
+bool same_case(const vpd_case &a, const vpd_case &b) {
+#define VPD_SAME(f) (std::memcmp(&a.f, &b.f, sizeof(a.f)) == 0)
+  return VPD_SAME(nx) && VPD_SAME(ny) && VPD_SAME(nz) && VPD_SAME(spacing) && VPD_SAME(horizon) &&
+         VPD_SAME(jitter) && VPD_SAME(jitter_seed) && VPD_SAME(dt) && VPD_SAME(density) && VPD_SAME(bc_mode) &&
+         VPD_SAME(load_axis) && VPD_SAME(region_layers) && VPD_SAME(plane_strain) && VPD_SAME(amplitude) &&
+         VPD_SAME(rise_time) && VPD_SAME(grip_velocity) && VPD_SAME(ramp_time) && VPD_SAME(observation_min) &&
+         VPD_SAME(observation_max) && VPD_SAME(props) && VPD_SAME(nstatev) && VPD_SAME(reference_temperature) &&
+         VPD_SAME(damage_mode) && VPD_SAME(damage_initiation) && VPD_SAME(damage_failure) &&
+         VPD_SAME(precision) && VPD_SAME(material_mode) && VPD_SAME(damage_deletion);
+#undef VPD_SAME
+}
+
+CheckpointHeader checkpoint_header(vpd_handle *h, const std::vector<Section> &v) {
+  CheckpointHeader hd;
+  std::memset(&hd, 0, sizeof(hd));
+  std::memcpy(hd.magic, "VPDCKPT", 8);
+  hd.version = 1;
+  hd.sections = (uint32_t)v.size();
+  hd.step = h->step, hd.n = h->n, hd.nbonds = h->nbonds, hd.sell_total = h->sell_total;
+  hd.stencil_words = h->st.nw, hd.mixed = h->params.mixed;
+  hd.host_vumat = h->params.host_vumat != nullptr, hd.surrogate = h->params.surrogate;
+  for (const Section &sec : v)
+    hd.payload += sec.bytes;
+  hd.c = h->c;
+  return hd;
+}
+
 }  // namespace
 
 extern "C" {
@@ -718,6 +787,62 @@ int vpd_set_host_vumat(vpd_handle *h, const char *plugin_path, const char *symbo
   }
   return host_vumat_attach(h->params, plugin_path, symbol, cmname, props, nprops, nstatev, density, h->c.spacing,
                            h->c.reference_temperature, h->stream);
+}
+
+int64_t vpd_checkpoint_bytes(vpd_handle *h) {
+  if (!h)
+    return -1;
+  const auto v = checkpoint_sections(h);
+  return (int64_t)(sizeof(CheckpointHeader) + checkpoint_header(h, v).payload);
+}
+
+int vpd_checkpoint_save(vpd_handle *h, void *buffer, int64_t bytes) {
+  if (!h || !buffer)
+    return set_error(VPD_ERR_INVALID, "vpd_checkpoint_save: null argument");
+  const auto v = checkpoint_sections(h);
+  const CheckpointHeader hd = checkpoint_header(h, v);
+  if (bytes != (int64_t)(sizeof(hd) + hd.payload))
+    return set_error(VPD_ERR_INVALID, "vpd_checkpoint_save: buffer size is not vpd_checkpoint_bytes");
+  char *out = static_cast<char *>(buffer);
+  std::memcpy(out, &hd, sizeof(hd));
+  size_t at = sizeof(hd);
+  for (const Section &sec : v) {
+    VPD_CUDA(cudaMemcpyAsync(out + at, sec.ptr, sec.bytes, cudaMemcpyDeviceToHost, h->stream));
+    at += sec.bytes;
+  }
+  VPD_CUDA(cudaStreamSynchronize(h->stream));
+  return VPD_OK;
+}
+
+int vpd_checkpoint_load(vpd_handle *h, const void *buffer, int64_t bytes) {
+  if (!h || !buffer)
+    return set_error(VPD_ERR_INVALID, "vpd_checkpoint_load: null argument");
+  const auto v = checkpoint_sections(h);
+  CheckpointHeader mine = checkpoint_header(h, v), theirs;
+  if (bytes < (int64_t)sizeof(theirs))
+    return set_error(VPD_ERR_INVALID, "vpd_checkpoint_load: buffer too small for a checkpoint");
+  std::memcpy(&theirs, buffer, sizeof(theirs));
+  if (std::memcmp(theirs.magic, "VPDCKPT", 8) != 0 || theirs.version != 1)
+    return set_error(VPD_ERR_INVALID, "vpd_checkpoint_load: not a checkpoint of this library");
+  mine.step = theirs.step;  // the one field the loading handle takes over
+  const bool case_matches = same_case(mine.c, theirs.c);
+  std::memset(&mine.c, 0, sizeof(mine.c));
+  std::memset(&theirs.c, 0, sizeof(theirs.c));
+  if (!case_matches || std::memcmp(&mine, &theirs, sizeof(mine)) != 0)
+    return set_error(VPD_ERR_INVALID, "vpd_checkpoint_load: the checkpoint was saved from a handle with another "
+                                      "case, layout, precision or material path");
+  if (bytes != (int64_t)(sizeof(theirs) + theirs.payload))
+    return set_error(VPD_ERR_INVALID, "vpd_checkpoint_load: buffer size does not match the checkpoint");
+  VPD_CUDA(cudaStreamSynchronize(h->stream));
+  const char *in = static_cast<const char *>(buffer);
+  size_t at = sizeof(theirs);
+  for (const Section &sec : v) {
+    VPD_CUDA(cudaMemcpyAsync(sec.ptr, in + at, sec.bytes, cudaMemcpyHostToDevice, h->stream));
+    at += sec.bytes;
+  }
+  VPD_CUDA(cudaStreamSynchronize(h->stream));
+  h->step = theirs.step;
+  return VPD_OK;
 }
 
 int vpd_profile_increment(vpd_handle *h, int32_t nsteps, double *stage_ms) {

@@ -94,6 +94,10 @@ def library():
                                         ctypes.POINTER(SurrogateReport)]
     lib.vpd_set_surrogate.argtypes = [_VP, _VP, _VP, ctypes.c_int32, ctypes.c_int32]
     lib.vpd_mlp_gradients.argtypes = [_VP, _VP, _VP, _VP, ctypes.c_int64, _VP, _VP]
+    lib.vpd_checkpoint_bytes.argtypes = [_VP]
+    lib.vpd_checkpoint_bytes.restype = ctypes.c_int64
+    lib.vpd_checkpoint_save.argtypes = [_VP, _VP, ctypes.c_int64]
+    lib.vpd_checkpoint_load.argtypes = [_VP, _VP, ctypes.c_int64]
     lib.vpd_set_host_vumat.argtypes = [_VP, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, _VP,
                                        ctypes.c_int32, ctypes.c_int32, ctypes.c_double]
     _lib = lib
@@ -213,6 +217,19 @@ class Simulation:
         _check(library().vpd_set_host_vumat(self._h, os.fsencode(plugin_path), symbol.encode(),
                                             cmname.encode(), pr.ctypes.data_as(_VP), pr.size,
                                             nstatev, density))
+
+    def checkpoint(self) -> bytes:
+        """The state this simulation carries into its next increment (vpd_checkpoint_save)."""
+        lib = library()
+        size = lib.vpd_checkpoint_bytes(self._h)
+        buf = ctypes.create_string_buffer(size)
+        _check(lib.vpd_checkpoint_save(self._h, buf, size))
+        return buf.raw
+
+    def restore(self, data: bytes):
+        """Continues from a checkpoint of a simulation of the same case (vpd_checkpoint_load)."""
+        buf = ctypes.create_string_buffer(bytes(data), len(data))
+        _check(library().vpd_checkpoint_load(self._h, buf, len(data)))
 
     def last_step_ms(self) -> float:
         out = ctypes.c_double()
