@@ -142,3 +142,39 @@ def test_runner_refuses_unknown_case_types(tmp_path, capsys):
     p.write_text(json.dumps({"name": "x", "type": "vumat_pd_demo"}))
     assert main([str(p)]) == 1
     assert "Unsupported case type" in capsys.readouterr().err
+
+
+# the reference's tests/config_rejection_test.py cases, through this runner's command line
+REJECTED_MATERIALS = [
+    ({"kinematicsMode": "legacy_small_strain"}, "Unsupported kinematicsMode"),
+    ({"internalIndicator": {"indices": [1], "reduction": "sum"}}, "reduction must be"),
+    ({"internalIndicator": {"indices": [1], "transform": "unknown"}}, "transform must be"),
+    ({"initialState": [0.0], "initialStateOverrides": {"5": 1.0}}, "initialState length"),
+    ({"equivalentPlasticStrainIndex": -2}, "outside nstatev"),
+    ({"internalIndicator": {"indices": [1.5]}}, "nonnegative integer"),
+    ({"internalIndicator": {"indices": ["1"]}}, "nonnegative integer"),
+    ({"initialStateOverrides": {"1junk": 1.0}}, "Invalid initialStateOverrides index"),
+    ({"initialState": [0.0, "bad", 0.0, 0.0, 0.0, 0.0, 0.0]}, "Expected numeric entries"),
+    ({"initialState": "not an array"}, "Expected numeric array"),
+    ({"internalIndicator": {"indices": "1"}}, "Expected integer array"),
+]
+REJECTED_TIMES = [("steps", 1.5, "representable integer"), ("steps", 2147483648, "representable integer"),
+                  ("dt", 0.0, "dt > 0"), ("dt", -1.0, "dt > 0"), ("dt", 1.0e308, "duration must be finite")]
+
+
+@pytest.mark.parametrize("edit, message",
+                         [((lambda c, e=e: c["materials"][0].update(e)), m) for e, m in REJECTED_MATERIALS]
+                         + [((lambda c, f=f, v=v: c["time_integration"].update({f: v})), m)
+                            for f, v, m in REJECTED_TIMES])
+def test_reference_config_rejections(tmp_path, capsys, edit, message):
+    from vpd.runner import main
+    with open(golden("examples/jc_material_point.json")) as f:
+        case = json.load(f)
+    edit(case)
+    out = tmp_path / "must_not_run"
+    case["output"]["directory"] = str(out)
+    p = tmp_path / "invalid.json"
+    p.write_text(json.dumps(case))
+    assert main([str(p), "--config-root", golden("")]) == 1
+    assert message in capsys.readouterr().err
+    assert not out.exists()

@@ -72,10 +72,47 @@ class AffineCase:
 
 
 def _num(obj, key, default):
+    """getDouble (SimpleJson.cpp:281-291)."""
     value = obj.get(key, default)
     if isinstance(value, bool) or not isinstance(value, (int, float)):
-        raise ValueError(f"{key} must be a number")
+        raise ValueError("Expected numeric field: " + key)
     return value
+
+
+def _int(obj, key, default):
+    """getInt (SimpleJson.cpp:264-279): a number with an exact 32-bit integer value."""
+    value = _num(obj, key, default)
+    if not math.isfinite(value) or math.trunc(value) != value or not -2**31 <= value <= 2**31 - 1:
+        raise ValueError("Expected representable integer field: " + key)
+    return int(value)
+
+
+def _double_array(obj, key):
+    """loadOptionalDoubleArray (DemoConfig.cpp:173-187)."""
+    if key not in obj:
+        return []
+    value = obj[key]
+    if not isinstance(value, list):
+        raise ValueError("Expected numeric array: " + key)
+    if any(isinstance(v, bool) or not isinstance(v, (int, float)) for v in value):
+        raise ValueError("Expected numeric entries in " + key)
+    return [float(v) for v in value]
+
+
+def _int_array(obj, key):
+    """loadOptionalIntArray (DemoConfig.cpp:189-204): non-negative integers."""
+    if key not in obj:
+        return []
+    value = obj[key]
+    if not isinstance(value, list):
+        raise ValueError("Expected integer array: " + key)
+    out = []
+    for v in value:
+        if isinstance(v, bool) or not isinstance(v, (int, float)) or not math.isfinite(v) \
+                or math.trunc(v) != v or v < 0 or v > 2**31 - 1:
+            raise ValueError("Expected nonnegative integer entries in " + key)
+        out.append(int(v))
+    return out
 
 
 def _load_material(entry, config_root, plugin_dir) -> PointMaterial:
@@ -91,25 +128,28 @@ def _load_material(entry, config_root, plugin_dir) -> PointMaterial:
         raise ValueError("JSON case hosts require corotational stress; use the dedicated spatial demo.")
     if entry.get("kinematicsMode", "corotational") != "corotational":
         raise ValueError("Unsupported kinematicsMode for material: " + label)
-    state = [float(v) for v in entry.get("initialState", [])]
+    state = _double_array(entry, "initialState")
     if state and len(state) != config.nstatev:
         raise ValueError("initialState length does not match nstatev.")
+    eqps = _int(entry, "equivalentPlasticStrainIndex", -1)
+    if not -1 <= eqps < config.nstatev:
+        raise ValueError("equivalentPlasticStrainIndex is outside nstatev for material: " + label)
     overrides = entry.get("initialStateOverrides")
     if isinstance(overrides, dict):
         if not state:
             state = [0.0] * config.nstatev
         for key, value in overrides.items():
-            if not key.isdigit() or not 0 <= int(key) < config.nstatev or isinstance(value, bool) \
-                    or not isinstance(value, (int, float)):
+            if not key or not all("0" <= ch <= "9" for ch in key):
+                raise ValueError("Invalid initialStateOverrides index for material: " + label)
+            if not int(key) < config.nstatev or isinstance(value, bool) or not isinstance(value, (int, float)):
                 raise ValueError("Invalid initialStateOverrides entry for material: " + label)
             state[int(key)] = float(value)
-    eqps = int(_num(entry, "equivalentPlasticStrainIndex", -1))
-    if not -1 <= eqps < config.nstatev:
-        raise ValueError("equivalentPlasticStrainIndex is outside nstatev for material: " + label)
+    if state and len(state) != config.nstatev:
+        raise ValueError("initialState length does not match nstatev for material: " + label)
     indices, reduction, transform = [], "max", "identity"
     indicator = entry.get("internalIndicator")
     if isinstance(indicator, dict):
-        indices = [int(i) for i in indicator.get("indices", [])]
+        indices = _int_array(indicator, "indices")
         reduction = indicator.get("reduction", "max")
         transform = indicator.get("transform", "identity")
         if reduction not in ("min", "max"):
@@ -155,9 +195,9 @@ def load_affine_case(path: str, kind: str, config_root: str | None = None,
         raise ValueError("PD geometry requires positive spacing and horizon.")
     if geo.get("type", "patch") != "patch":
         raise ValueError("Unsupported geometry type: " + str(geo.get("type")))
-    if min(_num(geo, k, 1) for k in ("nx", "ny", "nz")) < 2:
+    if min(_int(geo, k, 1) for k in ("nx", "ny", "nz")) < 2:
         raise ValueError("PD patch geometry requires nx/ny/nz >= 2.")
-    steps, dt = int(_num(ti, "steps", 1)), float(_num(ti, "dt", 1.0e-6))
+    steps, dt = _int(ti, "steps", 1), float(_num(ti, "dt", 1.0e-6))
     if steps < 1 or not math.isfinite(dt) or dt <= 0.0:
         raise ValueError("time_integration requires steps >= 1 and dt > 0.")
     total = float(_num(ti, "totalTime", 0.0))
@@ -190,8 +230,8 @@ def load_affine_case(path: str, kind: str, config_root: str | None = None,
         runs.append(_load_material(entry, config_root, plugin_dir))
     if not runs:
         raise ValueError("Demo case requires at least one material.")
-    return AffineCase(name=name, scope=root.get("scope", ""), nx=int(_num(geo, "nx", 1)),
-                      ny=int(_num(geo, "ny", 1)), nz=int(_num(geo, "nz", 1)),
+    return AffineCase(name=name, scope=root.get("scope", ""), nx=_int(geo, "nx", 1),
+                      ny=_int(geo, "ny", 1), nz=_int(geo, "nz", 1),
                       spacing=float(_num(geo, "spacing", 1.0)), horizon=float(_num(geo, "horizon", 1.0)),
                       steps=steps, dt=dt, mode=mode, max_strain=float(max_strain),
                       reference_stress_tolerance=float(_num(tol, "referenceStressAbsolute", 1.0e-6)),
