@@ -37,6 +37,17 @@ def test_jc_material_point_reproduces_reference_output(tmp_path):
         assert (tmp_path / name).read_bytes() == fixture("jc_material_point", name), name
 
 
+def test_bisection_tree_blocks_reproduce_reference_output(tmp_path):
+    """The plane-strain bisection evaluated 8 levels per plugin call (the GPU library's
+    setting) with the restated plugin: the same bytes as the reference CLI's sequential run."""
+    rc = run_material_point_case(golden("examples/jc_material_point.json"), str(tmp_path),
+                                 config_root=golden(""), plugin_dir=O.REF_DIR, log=lambda *a: None,
+                                 tree_levels=8)
+    assert rc == 0
+    for name in ("timeseries.csv", "metadata.json"):
+        assert (tmp_path / name).read_bytes() == fixture("jc_material_point", name), name
+
+
 def reference_cli(tmp_path, case):
     """Runs the reference CLI on a case dict; returns its output directory."""
     work = tmp_path / "ref"

@@ -20,7 +20,9 @@ import json
 import math
 import os
 
-from .vumat_plugin import PointInput, VumatPlugin, load_vumat_config
+import numpy as np
+
+from .vumat_plugin import PointInput, PointResult, VumatPlugin, load_vumat_config
 
 TIMESERIES_HEADER = ("material,step,time,applied_strain,stress,elastic_reference_stress,"
                      "reference_error,state_indicator,internal_energy,inelastic_energy,"
@@ -278,9 +280,119 @@ def _finite(values) -> bool:
     return all(math.isfinite(v) for v in values)
 
 
-def run_material(case: AffineCase, m: PointMaterial, lines: list) -> dict:
-    """runMaterial (:73-183) for one material; appends its timeseries lines."""
+def _trials(plugin: VumatPlugin, inp: PointInput, previous_lateral: float, laterals) -> list:
+    """The plugin on one row per trial lateral strain (the evaluate lambda of :117-125), all
+    rows in one block call; each row is computed independently of the others."""
+    rows = len(laterals)
+
+    def tile(values):
+        return np.tile(np.asarray(values, dtype=np.float64), (rows, 1))
+
+    lat = np.asarray(laterals, dtype=np.float64)
+    strain_rate, strain_n = tile(inp.strain_rate), tile(inp.strain_n)
+    defgrad_old, defgrad_new = tile(inp.defgrad_old), tile(inp.defgrad_new)
+    strain_rate[:, 4] = (lat - previous_lateral) / inp.dt
+    strain_n[:, 4] = previous_lateral
+    defgrad_old[:, 4] = 1.0 + previous_lateral
+    defgrad_new[:, 4] = 1.0 + lat
+    r = plugin.update_block(dt=inp.dt, step_time=inp.step_time, total_time=inp.total_time,
+                            char_length=np.full(rows, inp.char_length),
+                            temperature=np.full(rows, inp.temperature), strain_rate=strain_rate,
+                            rel_spin=tile(inp.rel_spin), stress_n=tile(inp.stress_n),
+                            stretch_old=tile(inp.stretch_old), stretch_new=tile(inp.stretch_new),
+                            defgrad_old=defgrad_old, defgrad_new=defgrad_new,
+                            state_old=tile(inp.state_old).reshape(rows, -1),
+                            internal_energy_old=np.full(rows, inp.internal_energy_old),
+                            inelastic_energy_old=np.full(rows, inp.inelastic_energy_old))
+    return [PointResult(stress=r["stress"][k].tolist(), state=r["state"][k].tolist(),
+                        temperature=float(r["temperature"][k]),
+                        internal_energy=float(r["internal_energy"][k]),
+                        inelastic_energy=float(r["inelastic_energy"][k])) for k in range(rows)]
+
+
+# levels of the bisection tree per plugin call: 8 (255 rows in one block) when the plugin is
+# this package's library, whose rows run in parallel on the GPU and whose cost is the round
+# trip; 1 for a host plugin, which would compute every speculative row
+TREE_LEVELS_DEVICE = 8
+
+
+def _plane_strain_bisection(plugin: VumatPlugin, inp: PointInput, load: float, previous_lateral: float,
+                            tree_levels: int):
+    """The reference's bisection on the lateral strain for zero lateral stress (:126-150),
+    evaluated ``tree_levels`` levels at a time. The interval of every node of the bisection tree
+    follows from the path alone (midpoint 0.5 (lower + upper), left keeps lower, right keeps
+    upper), so the next levels' midpoints go to the plugin as one block; the walk down the
+    tree then takes the reference's branch at each node from the residuals. It visits the
+    reference's midpoints with the same values and stops where it stops, so the lateral
+    strain and the result are the reference's; the other nodes' rows are discarded."""
+    lower, upper = -load, 0.25 * load
+    if tree_levels == 1:  # one midpoint per call, as the reference runs it
+        def evaluate(trial_lateral):
+            trial = inp.copy()
+            trial.strain_rate[4] = (trial_lateral - previous_lateral) / inp.dt
+            trial.strain_n[4] = previous_lateral
+            trial.defgrad_old[4] = 1.0 + previous_lateral
+            trial.defgrad_new[4] = 1.0 + trial_lateral
+            return plugin.update_point(trial)
+
+        lower_residual = evaluate(lower).stress[4]
+        upper_residual = evaluate(upper).stress[4]
+        if lower_residual * upper_residual > 0.0:
+            raise RuntimeError("Could not bracket zero lateral stress in material-point reference.")
+        lateral, result = 0.0, None
+        for _ in range(36):
+            lateral = 0.5 * (lower + upper)
+            result = evaluate(lateral)
+            residual = result.stress[4]
+            if abs(residual) < 1.0e-8:
+                break
+            if lower_residual * residual <= 0.0:
+                upper, upper_residual = lateral, residual
+            else:
+                lower, lower_residual = lateral, residual
+        return lateral, result
+    bracket = _trials(plugin, inp, previous_lateral, [lower, upper])
+    lower_residual, upper_residual = bracket[0].stress[4], bracket[1].stress[4]
+    if lower_residual * upper_residual > 0.0:
+        raise RuntimeError("Could not bracket zero lateral stress in material-point reference.")
+    lateral, result, iteration = 0.0, None, 0
+    while iteration < 36:
+        levels = min(tree_levels, 36 - iteration)
+        nodes = [(lower, upper)]  # heap order: node k has children 2k+1 (left) and 2k+2 (right)
+        mids = []
+        for k in range((1 << levels) - 1):
+            lo, up = nodes[k]
+            mid = 0.5 * (lo + up)
+            mids.append(mid)
+            if 2 * k + 2 < (1 << levels) - 1:
+                nodes.append((lo, mid))
+                nodes.append((mid, up))
+        results = _trials(plugin, inp, previous_lateral, mids)
+        k = 0
+        for _ in range(levels):
+            lateral, result = mids[k], results[k]
+            residual = result.stress[4]
+            iteration += 1
+            if abs(residual) < 1.0e-8:
+                return lateral, result
+            if lower_residual * residual <= 0.0:
+                upper, upper_residual = lateral, residual
+                k = 2 * k + 1
+            else:
+                lower, lower_residual = lateral, residual
+                k = 2 * k + 2
+    return lateral, result
+
+
+def run_material(case: AffineCase, m: PointMaterial, lines: list, tree_levels: int | None = None) -> dict:
+    """runMaterial (:73-183) for one material; appends its timeseries lines. ``tree_levels``
+    (default: by the plugin, see TREE_LEVELS_DEVICE) sets the bisection levels per call."""
+    from . import library_path
     plugin = VumatPlugin(m.config)
+    if tree_levels is None:
+        tree_levels = TREE_LEVELS_DEVICE if m.config.plugin_path == library_path() else 1
+    if not 1 <= tree_levels <= 8:
+        raise ValueError("tree_levels must be in [1, 8]")
     dt = case.dt
     inp = PointInput(dt=dt, char_length=case.spacing, temperature=m.reference_temperature,
                      state_old=list(m.initial_state) if m.initial_state else [0.0] * m.config.nstatev)
@@ -311,29 +423,7 @@ def run_material(case: AffineCase, m: PointMaterial, lines: list) -> dict:
             inp.defgrad_new[0] = 1.0 + load
         lateral = 0.0
         if case.mode == "plane_strain_x_uniaxial_stress":
-            def evaluate(trial_lateral):
-                trial = inp.copy()
-                trial.strain_rate[4] = (trial_lateral - previous_lateral) / dt
-                trial.strain_n[4] = previous_lateral
-                trial.defgrad_old[4] = 1.0 + previous_lateral
-                trial.defgrad_new[4] = 1.0 + trial_lateral
-                return plugin.update_point(trial)
-
-            lower, upper = -load, 0.25 * load
-            lower_residual = evaluate(lower).stress[4]
-            upper_residual = evaluate(upper).stress[4]
-            if lower_residual * upper_residual > 0.0:
-                raise RuntimeError("Could not bracket zero lateral stress in material-point reference.")
-            for _ in range(36):
-                lateral = 0.5 * (lower + upper)
-                result = evaluate(lateral)
-                residual = result.stress[4]
-                if abs(residual) < 1.0e-8:
-                    break
-                if lower_residual * residual <= 0.0:
-                    upper, upper_residual = lateral, residual
-                else:
-                    lower, lower_residual = lateral, residual
+            lateral, result = _plane_strain_bisection(plugin, inp, load, previous_lateral, tree_levels)
             previous_lateral = lateral
         else:
             result = plugin.update_point(inp)
@@ -380,13 +470,13 @@ def metadata_text(case: AffineCase, summaries: list, passed: bool) -> str:
 
 
 def run_material_point_case(path: str, out_dir: str | None = None, config_root: str | None = None,
-                            plugin_dir: str | None = None, log=print) -> int:
+                            plugin_dir: str | None = None, log=print, tree_levels: int | None = None) -> int:
     """Runs the case and writes its files; 0 when it passes, 2 when it does not (:185-234)."""
     case = load_point_case(path, config_root, plugin_dir)
     out = out_dir or case.output_directory
     os.makedirs(out, exist_ok=True)
     lines = [TIMESERIES_HEADER]
-    summaries = [run_material(case, m, lines) for m in case.materials]
+    summaries = [run_material(case, m, lines, tree_levels) for m in case.materials]
     passed = True
     for s in summaries:
         passed = passed and s["finite"]

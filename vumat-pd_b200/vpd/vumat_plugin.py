@@ -102,6 +102,18 @@ def load_vumat_config(path: str, plugin_dir: str | None = None) -> VumatConfig:
                        props=tuple(float(p) for p in props), density=density, stress_frame=frame)
 
 
+def _voigt(t):  # fullTensorToVumatVoigt, TensorVoigtMap.cpp:9-16
+    return (t[0], t[4], t[8], 0.5 * (t[5] + t[7]), 0.5 * (t[2] + t[6]), 0.5 * (t[1] + t[3]))
+
+
+def _full(v):  # vumatVoigtToFullTensor, TensorVoigtMap.cpp:18-20
+    return [v[0], v[5], v[4], v[5], v[1], v[3], v[4], v[3], v[2]]
+
+
+def _defgrad(t):  # fullTensorToVumatDefgrad, TensorVoigtMap.cpp:22-24
+    return (t[0], t[4], t[8], t[1], t[5], t[6], t[3], t[7], t[2])
+
+
 def _voigt_rows(t):
     """fullTensorToVumatVoigt (TensorVoigtMap.cpp:9-16) of each row of t [nb, 9] -> [6, nb]."""
     return np.stack([t[:, 0], t[:, 4], t[:, 8], 0.5 * (t[:, 5] + t[:, 7]), 0.5 * (t[:, 2] + t[:, 6]),
@@ -224,22 +236,45 @@ class VumatPlugin:
                     internal_energy=ei_new, inelastic_energy=ep_new)
 
     def update_point(self, p: PointInput) -> PointResult:
-        """One point through the plugin: updatePoint as a one-row block (:116-147)."""
+        """One point through the plugin: updatePoint as a one-row block (:116-147), packed
+        directly (a host loop calls it once per evaluation)."""
+        c = self.config
         if not (math.isfinite(p.dt) and p.dt > 0.0):
             raise ValueError("VUMAT update requires dt > 0.")
-        if len(p.state_old) != self.config.nstatev:
+        if len(p.state_old) != c.nstatev:
             raise ValueError("stateOld entry size does not match nstatev.")
-        row = lambda t: np.array([t], dtype=np.float64)  # noqa: E731
-        r = self.update_block(dt=p.dt, step_time=p.step_time, total_time=p.total_time,
-                              char_length=[p.char_length], temperature=[p.temperature],
-                              strain_rate=row(p.strain_rate), rel_spin=row(p.rel_spin),
-                              stress_n=row(p.stress_n), stretch_old=row(p.stretch_old),
-                              stretch_new=row(p.stretch_new), defgrad_old=row(p.defgrad_old),
-                              defgrad_new=row(p.defgrad_new),
-                              state_old=np.array([p.state_old], dtype=np.float64).reshape(1, -1),
-                              internal_energy_old=[p.internal_energy_old],
-                              inelastic_energy_old=[p.inelastic_energy_old])
-        return PointResult(stress=r["stress"][0].tolist(), state=r["state"][0].tolist(),
-                           temperature=float(r["temperature"][0]),
-                           internal_energy=float(r["internal_energy"][0]),
-                           inelastic_energy=float(r["inelastic_energy"][0]))
+
+        def arr(values):
+            return np.array(values, dtype=np.float64)
+
+        field_cols, state_cols = max(1, c.nfieldv), max(1, c.nstatev)
+        stress_old = arr(_voigt(p.stress_n))
+        strain_inc = arr([v * p.dt for v in _voigt(p.strain_rate)])
+        spin = arr((p.rel_spin[5], p.rel_spin[6], p.rel_spin[1]))
+        stretch_old, stretch_new = arr(_voigt(p.stretch_old)), arr(_voigt(p.stretch_new))
+        defgrad_old, defgrad_new = arr(_defgrad(p.defgrad_old)), arr(_defgrad(p.defgrad_new))
+        state_old = np.zeros(state_cols)
+        state_old[:c.nstatev] = p.state_old
+        temp_old, temp_new = arr([p.temperature]), arr([p.temperature])
+        ei_old, ep_old = arr([p.internal_energy_old]), arr([p.inelastic_energy_old])
+        ei_new, ep_new = arr([p.internal_energy_old]), arr([p.inelastic_energy_old])
+        stress_new, state_new = np.zeros(6), np.zeros(state_cols)
+        coord, char_length, density = np.zeros(3), arr([p.char_length]), arr([c.density])
+        field_old, field_new = np.zeros(field_cols), np.zeros(field_cols)
+        props = self._props.copy()
+        ints = [ctypes.c_int(v) for v in (1, 3, 3, c.nstatev, c.nfieldv, len(c.props), 0)]
+        times = [ctypes.c_double(v) for v in (p.step_time, p.total_time, p.dt)]
+
+        def dp(a):
+            return a.ctypes.data_as(_DP)
+
+        self._call(*[ctypes.byref(v) for v in ints], *[ctypes.byref(v) for v in times],
+                   ctypes.create_string_buffer(self._cmname, 80),
+                   dp(coord), dp(char_length), dp(props), dp(density), dp(strain_inc), dp(spin),
+                   dp(temp_old), dp(stretch_old), dp(defgrad_old), dp(field_old), dp(stress_old),
+                   dp(state_old), dp(ei_old), dp(ep_old), dp(temp_new), dp(stretch_new),
+                   dp(defgrad_new), dp(field_new), dp(stress_new), dp(state_new), dp(ei_new),
+                   dp(ep_new))
+        return PointResult(stress=_full(stress_new.tolist()), state=state_new[:c.nstatev].tolist(),
+                           temperature=float(temp_new[0]), internal_energy=float(ei_new[0]),
+                           inelastic_energy=float(ep_new[0]))
