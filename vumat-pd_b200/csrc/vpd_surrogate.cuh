@@ -1,6 +1,6 @@
 // The learned Johnson-Cook return map: input features, training targets and the Newton
 // acceptance that gates the network's plastic increment (no counterpart in the reference; the
-// VUMAT's bisection, jc_bisection, stays the fallback and the judge).
+// VUMAT's bisection, jc_bisection, stays the fallback, and its residual decides acceptance).
 //
 // For a point whose elastic trial state yields (the VUMAT's first bisection iteration, at
 // epInc = 0, leaves a residual of at least the tolerance E 1e-9), the plastic increment solves
