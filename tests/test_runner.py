@@ -208,3 +208,22 @@ def test_boundary_case_with_a_host_plugin(tmp_path):
     with pytest.raises(ValueError, match="must be 1 or -1"):
         load_boundary_case(str(p), golden(""), O.REF_DIR)
     assert load_boundary_case(case_path("pd_coarse.json"), golden("")).materials[0].host_plugin is None
+
+
+def test_runner_surrogate_option_checks(tmp_path):
+    """The surrogate replaces the device JC update only, and takes the library's guess names;
+    both are refused before any GPU work."""
+    import oracle as O
+    from vpd.runner import main, run_boundary_case
+    with open(case_path("pd_coarse.json")) as f:
+        d = json.load(f)
+    d["materials"][0].update(materialConfigPath="configs/elastic.json", equivalentPlasticStrainIndex=-1)
+    p = tmp_path / "case.json"
+    p.write_text(json.dumps(d))
+    with pytest.raises(ValueError, match="not a host plugin"):
+        run_boundary_case(str(p), str(tmp_path / "o"), golden(""), plugin_dir=O.REF_DIR, surrogate="hybrid")
+    with pytest.raises(ValueError, match="one of"):
+        run_boundary_case(case_path("pd_coarse.json"), str(tmp_path / "o"), golden(""), surrogate="fast")
+    with pytest.raises(SystemExit):
+        main([case_path("pd_coarse.json"), "--surrogate", "fast"])
+    assert not (tmp_path / "o").exists()

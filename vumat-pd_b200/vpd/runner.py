@@ -207,13 +207,25 @@ def plugin_file(m) -> str:
     return os.path.basename(m.host_plugin.plugin_path) if m.host_plugin is not None else "libvpd_gpu.so"
 
 
+SURROGATE_GUESSES = ("network", "hybrid", "warm_start")
+
+
 def run_boundary_case(path: str, out_dir: str = None, config_root: str = None, precision: int = None,
-                      log=print, plugin_dir: str = None) -> int:
+                      log=print, plugin_dir: str = None, surrogate: str = None) -> int:
     """Runs every material of a boundary-value case file and writes its three output files into
     ``out_dir`` (default: the case's output.directory). Returns 0 when every material passes
     the case's acceptance limits, 2 otherwise (the reference runner's exit status)."""
-    from . import Simulation
+    from . import Simulation, train_surrogate
+    from .case import MATERIAL_SURROGATE
     bc = load_boundary_case(path, config_root, plugin_dir)
+    if surrogate is not None:
+        if surrogate not in SURROGATE_GUESSES:
+            raise ValueError(f"surrogate {surrogate!r}: one of {', '.join(SURROGATE_GUESSES)}")
+        for m in bc.materials:
+            if m.host_plugin is not None:
+                raise ValueError(f"material {m.label}: the surrogate replaces the device Johnson-Cook "
+                                 "update, not a host plugin")
+    networks = {}  # trained once per set of Johnson-Cook props
     out = out_dir or bc.output_directory
     os.makedirs(out, exist_ok=True)
     summaries = []
@@ -223,6 +235,10 @@ def run_boundary_case(path: str, out_dir: str = None, config_root: str = None, p
         fs.write(SNAPSHOT_HEADER)
         for m in bc.materials:
             case = m.case if precision is None else m.case.replace(precision=precision)
+            if surrogate is not None:
+                case = case.replace(material_mode=MATERIAL_SURROGATE)
+                if surrogate != "warm_start" and case.props not in networks:
+                    networks[case.props] = train_surrogate(case.props)[:2]
             axis = case.load_axis
             started = time.perf_counter()
             chunks, done = [], 0
@@ -231,6 +247,9 @@ def run_boundary_case(path: str, out_dir: str = None, config_root: str = None, p
                     p = m.host_plugin
                     sim.set_host_vumat(p.plugin_path, p.props, p.nstatev, p.density, cmname=p.cmname,
                                        symbol=p.symbol)
+                if surrogate is not None:
+                    w, b = networks.get(case.props, (None, None))
+                    sim.set_surrogate(w, b, guess=surrogate, newton_steps=2)
                 x0 = sim.field("position")
                 lo, hi = observation_bounds(x0, axis, (case.region_layers - 1) * case.spacing,
                                             case.observation_min, case.observation_max)
@@ -274,6 +293,11 @@ def main(argv=None) -> int:
     ap.add_argument("--config-root", help="directory the material config paths are relative to")
     ap.add_argument("--plugin-dir", help="directory of the materials' VUMAT plugins (default: the "
                     "stock Johnson-Cook plugin is this package's GPU library)")
+    ap.add_argument("--precision", choices=("fp64", "mixed"), default="fp64",
+                    help="boundary-value cases: FP64 throughout (the drop-in), or FP32 bond sums")
+    ap.add_argument("--surrogate", choices=SURROGATE_GUESSES,
+                    help="boundary-value cases: the learned Johnson-Cook return map with this guess "
+                         "(the network is trained on the GPU first; the VUMAT stays the fallback)")
     args = ap.parse_args(argv)
     try:
         with open(args.case) as f:
@@ -286,7 +310,10 @@ def main(argv=None) -> int:
             return run_demo_case(args.case, args.out, args.config_root, args.plugin_dir)
         if kind != "vumat_pd_boundary_case":
             raise ValueError("Unsupported case type: " + str(kind))
-        return run_boundary_case(args.case, args.out, args.config_root, plugin_dir=args.plugin_dir)
+        from .case import PRECISION_FP64, PRECISION_MIXED
+        precision = PRECISION_MIXED if args.precision == "mixed" else PRECISION_FP64
+        return run_boundary_case(args.case, args.out, args.config_root, precision=precision,
+                                 plugin_dir=args.plugin_dir, surrogate=args.surrogate)
     except (ValueError, OSError, RuntimeError) as e:
         print(f"error: {e}", file=sys.stderr)
         return 1
