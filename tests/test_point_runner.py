@@ -189,3 +189,13 @@ def test_reference_config_rejections(tmp_path, capsys, edit, message):
     assert main([str(p), "--config-root", golden("")]) == 1
     assert message in capsys.readouterr().err
     assert not out.exists()
+
+
+def test_runner_command_line_runs_material_point_cases(tmp_path):
+    """``python -m vpd.runner`` dispatches on the case type: the material-point example through
+    the command line writes the reference CLI's files."""
+    from vpd.runner import main
+    rc = main([golden("examples/jc_material_point.json"), "--config-root", golden(""),
+               "--plugin-dir", O.REF_DIR, "--out", str(tmp_path)])
+    assert rc == 0
+    assert (tmp_path / "timeseries.csv").read_bytes() == fixture("jc_material_point", "timeseries.csv")
