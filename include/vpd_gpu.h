@@ -208,6 +208,11 @@ int vpd_last_step_ms(const vpd_handle *h, double *ms);
    device only.
    (No reference counterpart: per-stage timing of the step loop.) */
 int vpd_profile_increment(vpd_handle *h, int32_t nsteps, double *stage_ms);
+/* The VUMAT state every point starts from (VumatPdCorrespondenceMaterial::initialize with a
+   configured initialState, src/material/VumatPdCorrespondenceMaterial.cpp:62-66): state[0..
+   nstatev) for every point, the case's further components left at zero. Before the first
+   vpd_step; nstatev at most the case's. */
+int vpd_set_initial_state(vpd_handle *h, const double *state, int32_t nstatev);
 /* Checkpoint and resume between increments. A checkpoint holds the state one increment
    carries to the next: displacements, velocities, accelerations and forces; the material
    history (F, V, R, E, stress, state, energies); broken bonds; point damage and plugin

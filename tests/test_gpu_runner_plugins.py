@@ -1,12 +1,13 @@
-"""A boundary-value case file whose material is a user plugin (here the reference's linear
-elastic routine, restated in oracle/_ref) through ``python -m vpd.runner --plugin-dir``: the
-increments on the GPU around the host plugin path, against the reference's own CLI
-(oracle/_ref/vumat_pd_run, built from its sources, run here on the CPU) on the same file.
+"""Boundary-value case files through ``python -m vpd.runner`` on the GPU, against the
+reference's own CLI (oracle/_ref/vumat_pd_run, built from its sources, run here on the CPU) on
+the same file: a user plugin (the reference's linear elastic routine, restated in oracle/_ref)
+through the host plugin path, and the device Johnson-Cook update from a configured initial
+state.
 
 Both write the same rows and keys. The numbers agree within 1e-7 of each column's scale,
-because the GPU sums differ from the CPU's by rounding; the net internal force, rounding noise
-in both, stays under the case's 1e-6 N limit. The host plugin path matches the
-reference library within 1e-9 in test_gpu_host_vumat.py."""
+because the GPU sums differ from the CPU's by rounding. The net internal force is rounding
+noise in both, and it must stay under the case's 1e-6 N limit. The host plugin path matches
+the reference library within 1e-9 in test_gpu_host_vumat.py."""
 import csv
 import io
 import json
@@ -22,18 +23,22 @@ from conftest import golden
 import oracle as O
 from vpd.runner import run_boundary_case
 
-pytestmark = [pytest.mark.gpu, pytest.mark.late]
+pytestmark = [pytest.mark.gpu, pytest.mark.late, pytest.mark.skipif(
+    not os.path.exists(os.path.join(O.REF_DIR, "vumat_pd_run")), reason="reference CLI not built")]
 CLI = os.path.join(O.REF_DIR, "vumat_pd_run")
 
 
-@pytest.mark.skipif(not os.path.exists(CLI), reason="reference CLI not built")
-def test_elastic_plugin_boundary_case_matches_reference_cli(tmp_path):
+def pd_coarse_600(**material):
     with open(golden("cases/pd_coarse.json")) as f:
         case = json.load(f)
     dt = case["time_integration"]["dt"]
     case["time_integration"].update(steps=600, totalTime=600 * dt)
-    case["materials"][0].update(materialConfigPath="configs/elastic.json", equivalentPlasticStrainIndex=-1)
+    case["materials"][0].update(material)
     case["output"] = {"directory": "out"}
+    return case
+
+
+def compare_with_reference_cli(tmp_path, case, plugin_dir=None):
     work = tmp_path / "ref"
     shutil.copytree(golden("configs"), work / "configs")
     (work / "cases").mkdir()
@@ -41,7 +46,7 @@ def test_elastic_plugin_boundary_case_matches_reference_cli(tmp_path):
     path.write_text(json.dumps(case))
     ref = subprocess.run([CLI, "cases/case.json"], cwd=work, stdout=subprocess.DEVNULL)
     rc = run_boundary_case(str(path), str(tmp_path / "ours"), str(work), log=lambda *a: None,
-                           plugin_dir=O.REF_DIR)
+                           plugin_dir=plugin_dir)
     assert rc == ref.returncode
     for name in ("timeseries.csv", "field_snapshots.csv"):
         a = list(csv.reader(io.StringIO((tmp_path / "ours" / name).read_text())))
@@ -53,7 +58,7 @@ def test_elastic_plugin_boundary_case_matches_reference_cli(tmp_path):
                 continue
             x = np.array([float(r[c]) for r in a[1:]])
             y = np.array([float(r[c]) for r in b[1:]])
-            if col == "net_internal_force_N":  # rounding noise: under the case's 1e-6 N limit
+            if col == "net_internal_force_N":
                 assert np.abs(x).max() < 1e-6 and np.abs(y).max() < 1e-6
                 continue
             assert np.abs(x - y).max() <= 1e-7 * np.abs(y).max() + 1e-12, (name, col)
@@ -61,7 +66,20 @@ def test_elastic_plugin_boundary_case_matches_reference_cli(tmp_path):
     theirs = json.loads((work / "out" / "metadata.json").read_text())
     assert list(ours) == list(theirs)
     mo, mt = ours["materials"][0], theirs["materials"][0]
-    assert list(mo) == list(mt)
-    assert mo["plugin_file"] == mt["plugin_file"] == "elastic_vumat_plugin.so"
-    assert mo["status"] == mt["status"] and mo["maxEqps"] == mt["maxEqps"] == 0
+    assert list(mo) == list(mt) and mo["status"] == mt["status"]
     assert mo["finalReaction_N"] == pytest.approx(mt["finalReaction_N"], rel=1e-7)
+    return mo, mt
+
+
+def test_elastic_plugin_boundary_case_matches_reference_cli(tmp_path):
+    mo, mt = compare_with_reference_cli(
+        tmp_path, pd_coarse_600(materialConfigPath="configs/elastic.json", equivalentPlasticStrainIndex=-1),
+        O.REF_DIR)
+    assert mo["plugin_file"] == mt["plugin_file"] == "elastic_vumat_plugin.so"
+    assert mo["maxEqps"] == mt["maxEqps"] == 0
+
+
+def test_initial_state_boundary_case_matches_reference_cli(tmp_path):
+    """JC from an initialised state with 1 % plastic strain already accumulated."""
+    mo, mt = compare_with_reference_cli(tmp_path, pd_coarse_600(initialState=[1.0, 0.01, 293.0, 0.0, 0.0, 1.0]))
+    assert mo["maxEqps"] == pytest.approx(mt["maxEqps"], rel=1e-7) and mt["maxEqps"] > 0.01

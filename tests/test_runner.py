@@ -57,7 +57,9 @@ def test_pd_coarse_file_is_the_hand_written_case():
     (lambda d: d["boundary_conditions"].update(component="z"), "component"),
     (lambda d: d["damage"].update(model="bond_based"), "damage.model"),
     (lambda d: d.update(type="vumat_material_point_case"), "vumat_pd_boundary_case"),
-    (lambda d: d["materials"][0].update(initialStateOverrides={"1": 0.1}), "initialStateOverrides"),
+    (lambda d: d["materials"][0].update(internalIndicator={"indices": [1]}), "internalIndicator"),
+    (lambda d: d["materials"][0].update(initialStateOverrides={"1x": 0.1}), "initialStateOverrides index"),
+    (lambda d: d["materials"][0].update(initialState=[0.0, 0.1]), "initialState length"),
     (lambda d: d["materials"][0].update(materialConfigPath="configs/elastic.json"), "elastic.json"),
 ])
 def test_unsupported_case_files_are_refused(tmp_path, edit, message):
@@ -227,3 +229,18 @@ def test_runner_surrogate_option_checks(tmp_path):
     with pytest.raises(SystemExit):
         main([case_path("pd_coarse.json"), "--surrogate", "fast"])
     assert not (tmp_path / "o").exists()
+
+
+def test_initial_state_loads():
+    """initialState and its overrides give every point's starting state (DemoConfig.cpp:220-251)."""
+    with open(case_path("pd_coarse.json")) as f:
+        d = json.load(f)
+    d["materials"][0].update(initialStateOverrides={"1": 0.01, "2": 300.0})
+    import tempfile
+    with tempfile.TemporaryDirectory() as t:
+        p = os.path.join(t, "case.json")
+        with open(p, "w") as f:
+            json.dump(d, f)
+        m = load_boundary_case(p, golden("")).materials[0]
+    assert m.initial_state == (0.0, 0.01, 300.0, 0.0, 0.0, 0.0)
+    assert load_boundary_case(case_path("pd_coarse.json"), golden("")).materials[0].initial_state == ()

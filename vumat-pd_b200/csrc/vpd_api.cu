@@ -789,6 +789,26 @@ int vpd_set_host_vumat(vpd_handle *h, const char *plugin_path, const char *symbo
                            h->c.reference_temperature, h->stream);
 }
 
+int vpd_set_initial_state(vpd_handle *h, const double *state, int32_t nstatev) {
+  if (!h || (!state && nstatev > 0))
+    return set_error(VPD_ERR_INVALID, "vpd_set_initial_state: null argument");
+  if (h->step != 0)
+    return set_error(VPD_ERR_INVALID, "vpd_set_initial_state: call before the first vpd_step");
+  if (nstatev < 0 || nstatev > h->c.nstatev)
+    return set_error(VPD_ERR_INVALID, "Initial VUMAT state size does not match nstatev.");
+  for (int c = 0; c < nstatev; ++c)
+    if (!std::isfinite(state[c]))
+      return set_error(VPD_ERR_NONFINITE, "vpd_set_initial_state: non-finite state value");
+  std::vector<double> column((size_t)h->n);
+  VPD_CUDA(cudaStreamSynchronize(h->stream));
+  for (int c = 0; c < nstatev; ++c) {  // every point starts from the same state (:62-66)
+    std::fill(column.begin(), column.end(), state[c]);
+    VPD_CUDA(cudaMemcpy(h->state + (size_t)c * h->n, column.data(), sizeof(double) * column.size(),
+                        cudaMemcpyHostToDevice));
+  }
+  return VPD_OK;
+}
+
 int64_t vpd_checkpoint_bytes(vpd_handle *h) {
   if (!h)
     return -1;

@@ -94,6 +94,7 @@ def library():
                                         ctypes.POINTER(SurrogateReport)]
     lib.vpd_set_surrogate.argtypes = [_VP, _VP, _VP, ctypes.c_int32, ctypes.c_int32]
     lib.vpd_mlp_gradients.argtypes = [_VP, _VP, _VP, _VP, ctypes.c_int64, _VP, _VP]
+    lib.vpd_set_initial_state.argtypes = [_VP, _VP, ctypes.c_int32]
     lib.vpd_checkpoint_bytes.argtypes = [_VP]
     lib.vpd_checkpoint_bytes.restype = ctypes.c_int64
     lib.vpd_checkpoint_save.argtypes = [_VP, _VP, ctypes.c_int64]
@@ -217,6 +218,11 @@ class Simulation:
         _check(library().vpd_set_host_vumat(self._h, os.fsencode(plugin_path), symbol.encode(),
                                             cmname.encode(), pr.ctypes.data_as(_VP), pr.size,
                                             nstatev, density))
+
+    def set_initial_state(self, state):
+        """Every point's VUMAT state before the first step (vpd_set_initial_state)."""
+        st = np.ascontiguousarray(state, dtype=np.float64)
+        _check(library().vpd_set_initial_state(self._h, st.ctypes.data_as(_VP), st.size))
 
     def checkpoint(self) -> bytes:
         """The state this simulation carries into its next increment (vpd_checkpoint_save)."""

@@ -13,8 +13,8 @@ naming the field:
     y (``bottom``/``top``), rigid-body suppression on;
   * the stock Johnson-Cook plugin as the device update, or any other VUMAT plugin through the
     host plugin path (found in the plugin directory); the corotational stress frame, the
-    legacy_vumat_pd tensor convention, eqps at state variable 2 or none, no initial-state
-    overrides or internal indicator;
+    legacy_vumat_pd tensor convention, eqps at state variable 2 or none, an initial state
+    (``initialState``, ``initialStateOverrides``), no internal indicator;
   * damage ``none``, ``critical_stretch`` or the point modes ``eqps_threshold`` and
     ``max_principal_strain`` (with ``deletionEnabled``).
 """
@@ -40,6 +40,7 @@ class MaterialRun:
     eqps_index: int                  # state variable written as eqps (-1: none)
     source_density: float            # the material config's density (kg/m^3)
     host_plugin: object = None       # VumatConfig of a plugin run on the host (None: device JC)
+    initial_state: tuple = ()        # every point's starting VUMAT state (empty: zeros)
 
 
 @dataclasses.dataclass
@@ -113,6 +114,26 @@ def load_material_config(path: str, plugin_dir: str = None) -> dict:
     # columns the device layout has
     return {"props": (0.0,) * 14, "nstatev": max(6, cfg.nstatev), "density": cfg.density,
             "host_plugin": cfg}
+
+
+def _initial_state(entry: dict, label: str, nstatev: int) -> tuple:
+    """initialState and initialStateOverrides of a material entry (DemoConfig.cpp:220-251), with
+    the reference's checks and messages."""
+    from .point_runner import _double_array
+    state = _double_array(entry, "initialState")
+    if state and len(state) != nstatev:
+        raise ValueError("initialState length does not match nstatev.")
+    overrides = entry.get("initialStateOverrides")
+    if isinstance(overrides, dict):
+        if not state:
+            state = [0.0] * nstatev
+        for key, value in overrides.items():
+            if not key or not all("0" <= ch <= "9" for ch in key):
+                raise ValueError("Invalid initialStateOverrides index for material: " + label)
+            if not int(key) < nstatev or isinstance(value, bool) or not isinstance(value, (int, float)):
+                raise ValueError("Invalid initialStateOverrides entry for material: " + label)
+            state[int(key)] = float(value)
+    return tuple(state)
 
 
 def load_boundary_case(path: str, config_root: str = None, plugin_dir: str = None) -> BoundaryCase:
@@ -199,9 +220,8 @@ def load_boundary_case(path: str, config_root: str = None, plugin_dir: str = Non
         rel = _get(entry, "materialConfigPath", _get(entry, "configPath", _get(entry, "material_config_path", "", str), str), str)
         if not rel:
             raise ValueError(f"material {label}: materialConfigPath is required")
-        for key in ("initialState", "initialStateOverrides", "internalIndicator"):
-            if key in entry:
-                raise ValueError(f"material {label}: {key} is not supported on the device")
+        if "internalIndicator" in entry:
+            raise ValueError(f"material {label}: internalIndicator is not supported on the device")
         if _get(entry, "kinematicsMode", "corotational", str) != "corotational":
             raise ValueError(f"material {label}: kinematicsMode must be corotational")
         cfg = load_material_config(os.path.join(config_root or ".", rel), plugin_dir)
@@ -212,6 +232,7 @@ def load_boundary_case(path: str, config_root: str = None, plugin_dir: str = Non
         if eqps_index not in (-1, 1):
             raise ValueError(f"material {label}: the device reduces state variable 2 as eqps; "
                              "equivalentPlasticStrainIndex must be 1 or -1")
+        initial_state = _initial_state(entry, label, nstatev)
         case = Case(name=f"{name}/{label}", nx=nx, ny=ny, nz=nz, spacing=spacing, horizon=horizon,
                     dt=dt, steps=steps, density=density, props=cfg["props"],
                     bc_mode=BC_SMOOTH_DISPLACEMENT, load_axis=0 if component == "x" else 1,
@@ -223,7 +244,8 @@ def load_boundary_case(path: str, config_root: str = None, plugin_dir: str = Non
                     damage_deletion=deletion)
         runs.append(MaterialRun(label=label, case=case, elastic_e=_get(entry, "elasticE", 0.0, float),
                                 elastic_nu=_get(entry, "elasticNu", 0.0, float), eqps_index=eqps_index,
-                                source_density=cfg["density"], host_plugin=cfg["host_plugin"]))
+                                source_density=cfg["density"], host_plugin=cfg["host_plugin"],
+                                initial_state=initial_state))
     return BoundaryCase(
         name=name, classification=_get(root, "classification", "verification", str),
         scope=_get(root, "scope", "", str), steps=steps, dt=dt,

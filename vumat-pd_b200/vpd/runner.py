@@ -247,6 +247,8 @@ def run_boundary_case(path: str, out_dir: str = None, config_root: str = None, p
                     p = m.host_plugin
                     sim.set_host_vumat(p.plugin_path, p.props, p.nstatev, p.density, cmname=p.cmname,
                                        symbol=p.symbol)
+                if m.initial_state:
+                    sim.set_initial_state(m.initial_state)
                 if surrogate is not None:
                     w, b = networks.get(case.props, (None, None))
                     sim.set_surrogate(w, b, guess=surrogate, newton_steps=2)
