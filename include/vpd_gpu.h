@@ -213,6 +213,13 @@ int vpd_profile_increment(vpd_handle *h, int32_t nsteps, double *stage_ms);
    nstatev) for every point, the case's further components left at zero. Before the first
    vpd_step; nstatev at most the case's. */
 int vpd_set_initial_state(vpd_handle *h, const double *state, int32_t nstatev);
+/* The diagnostics' internal indicator (internalIndicator of a material entry,
+   BoundaryValueCaseRunner.cpp:93-107): per point the minimum (reduction_min 1) or maximum of
+   state variables indices[0..count), 1 minus that when one_minus is 1; the timeseries column
+   VPD_DIAG_MAX_INTERNAL_INDICATOR then carries the largest over the points and 0 (0 without
+   an indicator). count at most 8. */
+int vpd_set_internal_indicator(vpd_handle *h, const int32_t *indices, int32_t count, int32_t reduction_min,
+                               int32_t one_minus);
 /* Checkpoint and resume between increments. A checkpoint holds the state one increment
    carries to the next: displacements, velocities, accelerations and forces; the material
    history (F, V, R, E, stress, state, energies); broken bonds; point damage and plugin

@@ -83,3 +83,12 @@ def test_initial_state_boundary_case_matches_reference_cli(tmp_path):
     """JC from an initialised state with 1 % plastic strain already accumulated."""
     mo, mt = compare_with_reference_cli(tmp_path, pd_coarse_600(initialState=[1.0, 0.01, 293.0, 0.0, 0.0, 1.0]))
     assert mo["maxEqps"] == pytest.approx(mt["maxEqps"], rel=1e-7) and mt["maxEqps"] > 0.01
+
+
+@pytest.mark.parametrize("indicator", [{"indices": [1], "reduction": "max"},
+                                       {"indices": [1, 4], "reduction": "min", "transform": "one_minus"}])
+def test_internal_indicator_boundary_case_matches_reference_cli(tmp_path, indicator):
+    """The per-increment maximum of the indicator (k_indicator) and its per-point snapshot column."""
+    mo, mt = compare_with_reference_cli(tmp_path, pd_coarse_600(internalIndicator=indicator))
+    assert mo["maxInternalIndicator"] == pytest.approx(mt["maxInternalIndicator"], rel=1e-7)
+    assert mt["maxInternalIndicator"] > 0

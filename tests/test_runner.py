@@ -57,7 +57,8 @@ def test_pd_coarse_file_is_the_hand_written_case():
     (lambda d: d["boundary_conditions"].update(component="z"), "component"),
     (lambda d: d["damage"].update(model="bond_based"), "damage.model"),
     (lambda d: d.update(type="vumat_material_point_case"), "vumat_pd_boundary_case"),
-    (lambda d: d["materials"][0].update(internalIndicator={"indices": [1]}), "internalIndicator"),
+    (lambda d: d["materials"][0].update(internalIndicator={"indices": [1], "reduction": "sum"}), "reduction must be"),
+    (lambda d: d["materials"][0].update(internalIndicator={"indices": [6]}), "outside nstatev"),
     (lambda d: d["materials"][0].update(initialStateOverrides={"1x": 0.1}), "initialStateOverrides index"),
     (lambda d: d["materials"][0].update(initialState=[0.0, 0.1]), "initialState length"),
     (lambda d: d["materials"][0].update(materialConfigPath="configs/elastic.json"), "elastic.json"),
@@ -244,3 +245,23 @@ def test_initial_state_loads():
         m = load_boundary_case(p, golden("")).materials[0]
     assert m.initial_state == (0.0, 0.01, 300.0, 0.0, 0.0, 0.0)
     assert load_boundary_case(case_path("pd_coarse.json"), golden("")).materials[0].initial_state == ()
+
+
+def test_internal_indicator_values():
+    """internalIndicator (BoundaryValueCaseRunner.cpp:93-107): min or max over the chosen state
+    variables, NaN skipped as std::min/std::max skip their second argument, then one_minus;
+    no clamp at 0 here (the per-step maximum starts at 0 on the device)."""
+    from vpd.boundary_case import indicator_values
+    state = np.array([[0.0, 0.2, 0.5], [0.0, np.nan, 0.1], [0.0, -0.3, -0.1]])
+    assert np.allclose(indicator_values(((1, 2), "max", "identity"), state), [0.5, 0.1, -0.1])
+    assert np.allclose(indicator_values(((1, 2), "min", "one_minus"), state), [0.8, 0.9, 1.3])
+    assert np.array_equal(indicator_values(None, state), np.zeros(3))
+    with open(case_path("pd_coarse.json")) as f:
+        d = json.load(f)
+    d["materials"][0]["internalIndicator"] = {"indices": [1], "reduction": "max"}
+    import tempfile
+    with tempfile.TemporaryDirectory() as t:
+        p = os.path.join(t, "case.json")
+        with open(p, "w") as f:
+            json.dump(d, f)
+        assert load_boundary_case(p, golden("")).materials[0].indicator == ((1,), "max", "identity")

@@ -789,6 +789,28 @@ int vpd_set_host_vumat(vpd_handle *h, const char *plugin_path, const char *symbo
                            h->c.reference_temperature, h->stream);
 }
 
+int vpd_set_internal_indicator(vpd_handle *h, const int32_t *indices, int32_t count, int32_t reduction_min,
+                               int32_t one_minus) {
+  if (!h || (!indices && count > 0))
+    return set_error(VPD_ERR_INVALID, "vpd_set_internal_indicator: null argument");
+  if (count < 0 || count > 8)
+    return set_error(VPD_ERR_UNSUPPORTED, "vpd_set_internal_indicator: at most 8 state variables");
+  for (int k = 0; k < count; ++k)
+    if (indices[k] < 0 || indices[k] >= h->c.nstatev)
+      return set_error(VPD_ERR_INVALID, "internalIndicator index is outside nstatev");
+  h->params.ind_count = count;
+  h->params.ind_min = reduction_min != 0;
+  h->params.ind_one_minus = one_minus != 0;
+  for (int k = 0; k < 8; ++k)
+    h->params.ind_idx[k] = k < count ? indices[k] : 0;
+  if (h->graph) {  // recaptured with the indicator's launch at the next vpd_step
+    VPD_CUDA(cudaStreamSynchronize(h->stream));
+    cudaGraphExecDestroy(h->graph);
+    h->graph = nullptr;
+  }
+  return VPD_OK;
+}
+
 int vpd_set_initial_state(vpd_handle *h, const double *state, int32_t nstatev) {
   if (!h || (!state && nstatev > 0))
     return set_error(VPD_ERR_INVALID, "vpd_set_initial_state: null argument");

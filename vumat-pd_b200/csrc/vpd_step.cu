@@ -20,6 +20,7 @@
 // blocks sums its group's share, and the last group sums the groups in order and writes the
 // increment's row.
 #include "vpd_math.cuh"
+#include <math_constants.h>
 #include "vpd_material.cuh"
 #include "vpd_step.cuh"
 
@@ -421,6 +422,45 @@ __global__ void __launch_bounds__(kBondThreads, 3) k_integrate(StepParams p) {
   *p.step = step + 1;
 }
 
+// ------------------------------------------------------------------ k_indicator
+// The case's internal indicator (internalIndicator, BoundaryValueCaseRunner.cpp:93-107,
+// :258-263): per point the min or max of the chosen state variables (optionally 1 - it), and
+// per increment the largest of them and 0, into the row k_integrate has just written (which
+// holds 0 there). Launched after k_integrate, only when the case configures an indicator.
+// The running value starts at 0 and takes no NaN (std::max keeps its first argument), so it is
+// never negative, and the IEEE bits of non-negative doubles order as the numbers: the blocks
+// combine with a 64-bit atomicMax.
+__global__ void __launch_bounds__(kBondThreads) k_indicator(const __grid_constant__ StepParams p) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  double v = 0.0;
+  if (i < p.n) {
+    double value = p.ind_min ? CUDART_INF : -CUDART_INF;
+    for (int k = 0; k < p.ind_count; ++k) {
+      const double item = p.state[(int64_t)p.ind_idx[k] * p.n + i];
+      value = p.ind_min ? (item < value ? item : value) : (value < item ? item : value);
+    }
+    if (p.ind_one_minus)
+      value = 1.0 - value;
+    v = v < value ? value : v;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const double w = __shfl_xor_sync(0xffffffffu, v, o);
+    v = v < w ? w : v;
+  }
+  __shared__ double warp_max[kBondThreads / 32];
+  if ((threadIdx.x & 31) == 0)
+    warp_max[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w)
+      v = v < warp_max[w] ? warp_max[w] : v;
+    const int64_t step = *p.step - 1;  // the increment k_integrate has just closed
+    double *slot = p.diag + (size_t)((step - 1) % kDiagRing) * VPD_DIAG_COLS + VPD_DIAG_MAX_INTERNAL_INDICATOR;
+    atomicMax(reinterpret_cast<unsigned long long *>(slot), (unsigned long long)__double_as_longlong(v));
+  }
+}
+
 // ------------------------------------------------------------------ set-up kernels
 // Constraints at t = 0 and the first displacement prediction (BoundaryValueCaseRunner.cpp:190,
 // then predictDisplacement + apply at t = dt).
@@ -543,6 +583,8 @@ int launch_stage(int stage, const StepParams &p, cudaStream_t s) {
     k_force<<<bond_grid(p.n), kBondThreads, 0, s>>>(p);
   } else {
     k_integrate<<<(unsigned)integrate_grid(p.n), kBondThreads, 0, s>>>(p);
+    if (p.ind_count)
+      k_indicator<<<(unsigned)((p.n + kBondThreads - 1) / kBondThreads), kBondThreads, 0, s>>>(p);
   }
   VPD_CUDA(cudaGetLastError());
   return VPD_OK;

@@ -98,6 +98,9 @@ struct StepParams {
   // VPD_DAMAGE_MAX_PRINCIPAL_STRAIN, 0 otherwise
   int point_damage, dmg_deletion;
   double *pdmg;               // damage per point, non-decreasing
+  // internal indicator of the diagnostics (vpd_set_internal_indicator; 0 indices: none)
+  int ind_count, ind_min, ind_one_minus;
+  int ind_idx[8];
   // device bookkeeping
   int64_t *step;              // increment being computed (1-based)
   unsigned int *status;

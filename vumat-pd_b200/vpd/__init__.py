@@ -95,6 +95,7 @@ def library():
     lib.vpd_set_surrogate.argtypes = [_VP, _VP, _VP, ctypes.c_int32, ctypes.c_int32]
     lib.vpd_mlp_gradients.argtypes = [_VP, _VP, _VP, _VP, ctypes.c_int64, _VP, _VP]
     lib.vpd_set_initial_state.argtypes = [_VP, _VP, ctypes.c_int32]
+    lib.vpd_set_internal_indicator.argtypes = [_VP, _VP, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]
     lib.vpd_checkpoint_bytes.argtypes = [_VP]
     lib.vpd_checkpoint_bytes.restype = ctypes.c_int64
     lib.vpd_checkpoint_save.argtypes = [_VP, _VP, ctypes.c_int64]
@@ -223,6 +224,12 @@ class Simulation:
         """Every point's VUMAT state before the first step (vpd_set_initial_state)."""
         st = np.ascontiguousarray(state, dtype=np.float64)
         _check(library().vpd_set_initial_state(self._h, st.ctypes.data_as(_VP), st.size))
+
+    def set_internal_indicator(self, indices, reduction: str = "max", transform: str = "identity"):
+        """The diagnostics' internal indicator (vpd_set_internal_indicator)."""
+        idx = np.ascontiguousarray(indices, dtype=np.int32)
+        _check(library().vpd_set_internal_indicator(self._h, idx.ctypes.data_as(_VP), idx.size,
+                                                    int(reduction == "min"), int(transform == "one_minus")))
 
     def checkpoint(self) -> bytes:
         """The state this simulation carries into its next increment (vpd_checkpoint_save)."""

@@ -14,7 +14,7 @@ naming the field:
   * the stock Johnson-Cook plugin as the device update, or any other VUMAT plugin through the
     host plugin path (found in the plugin directory); the corotational stress frame, the
     legacy_vumat_pd tensor convention, eqps at state variable 2 or none, an initial state
-    (``initialState``, ``initialStateOverrides``), no internal indicator;
+    (``initialState``, ``initialStateOverrides``) and the diagnostics' internal indicator;
   * damage ``none``, ``critical_stretch`` or the point modes ``eqps_threshold`` and
     ``max_principal_strain`` (with ``deletionEnabled``).
 """
@@ -24,6 +24,8 @@ import dataclasses
 import json
 import math
 import os
+
+import numpy as np
 
 from .vumat_plugin import load_vumat_config
 from .case import (BC_SMOOTH_DISPLACEMENT, DAMAGE_CRITICAL_STRETCH, DAMAGE_EQPS_THRESHOLD,
@@ -41,6 +43,7 @@ class MaterialRun:
     source_density: float            # the material config's density (kg/m^3)
     host_plugin: object = None       # VumatConfig of a plugin run on the host (None: device JC)
     initial_state: tuple = ()        # every point's starting VUMAT state (empty: zeros)
+    indicator: tuple = None          # (indices, reduction, transform) of internalIndicator
 
 
 @dataclasses.dataclass
@@ -136,6 +139,39 @@ def _initial_state(entry: dict, label: str, nstatev: int) -> tuple:
     return tuple(state)
 
 
+def _indicator(entry: dict, label: str, nstatev: int):
+    """internalIndicator of a material entry (DemoConfig.cpp:252-266), with the reference's checks."""
+    from .point_runner import _int_array
+    obj = entry.get("internalIndicator")
+    if not isinstance(obj, dict):
+        return None
+    indices = _int_array(obj, "indices")
+    reduction, transform = obj.get("reduction", "max"), obj.get("transform", "identity")
+    if reduction not in ("min", "max"):
+        raise ValueError("internalIndicator.reduction must be min or max.")
+    if transform not in ("identity", "one_minus"):
+        raise ValueError("internalIndicator.transform must be identity or one_minus.")
+    if any(not 0 <= i < nstatev for i in indices):
+        raise ValueError("internalIndicator index is outside nstatev for material: " + label)
+    if len(indices) > 8:
+        raise ValueError(f"material {label}: internalIndicator: at most 8 state variables on the device")
+    return (tuple(indices), reduction, transform) if indices else None
+
+
+def indicator_values(indicator, state: np.ndarray) -> np.ndarray:
+    """Per point the internal indicator of the state rows (BoundaryValueCaseRunner.cpp:93-107):
+    0 without one; else the min or max of the chosen variables (NaN skipped as std::min and
+    std::max skip it), 1 minus that for one_minus."""
+    if indicator is None:
+        return np.zeros(state.shape[0])
+    indices, reduction, transform = indicator
+    value = np.full(state.shape[0], np.inf if reduction == "min" else -np.inf)
+    for k in indices:
+        item = state[:, k]
+        value = np.where(item < value, item, value) if reduction == "min" else np.where(value < item, item, value)
+    return 1.0 - value if transform == "one_minus" else value
+
+
 def load_boundary_case(path: str, config_root: str = None, plugin_dir: str = None) -> BoundaryCase:
     """Reads a boundary-value case file. Material config paths are resolved against
     ``config_root`` (default: the current directory, as the reference's host resolves them),
@@ -220,8 +256,6 @@ def load_boundary_case(path: str, config_root: str = None, plugin_dir: str = Non
         rel = _get(entry, "materialConfigPath", _get(entry, "configPath", _get(entry, "material_config_path", "", str), str), str)
         if not rel:
             raise ValueError(f"material {label}: materialConfigPath is required")
-        if "internalIndicator" in entry:
-            raise ValueError(f"material {label}: internalIndicator is not supported on the device")
         if _get(entry, "kinematicsMode", "corotational", str) != "corotational":
             raise ValueError(f"material {label}: kinematicsMode must be corotational")
         cfg = load_material_config(os.path.join(config_root or ".", rel), plugin_dir)
@@ -233,6 +267,7 @@ def load_boundary_case(path: str, config_root: str = None, plugin_dir: str = Non
             raise ValueError(f"material {label}: the device reduces state variable 2 as eqps; "
                              "equivalentPlasticStrainIndex must be 1 or -1")
         initial_state = _initial_state(entry, label, nstatev)
+        indicator = _indicator(entry, label, nstatev)
         case = Case(name=f"{name}/{label}", nx=nx, ny=ny, nz=nz, spacing=spacing, horizon=horizon,
                     dt=dt, steps=steps, density=density, props=cfg["props"],
                     bc_mode=BC_SMOOTH_DISPLACEMENT, load_axis=0 if component == "x" else 1,
@@ -245,7 +280,7 @@ def load_boundary_case(path: str, config_root: str = None, plugin_dir: str = Non
         runs.append(MaterialRun(label=label, case=case, elastic_e=_get(entry, "elasticE", 0.0, float),
                                 elastic_nu=_get(entry, "elasticNu", 0.0, float), eqps_index=eqps_index,
                                 source_density=cfg["density"], host_plugin=cfg["host_plugin"],
-                                initial_state=initial_state))
+                                initial_state=initial_state, indicator=indicator))
     return BoundaryCase(
         name=name, classification=_get(root, "classification", "verification", str),
         scope=_get(root, "scope", "", str), steps=steps, dt=dt,

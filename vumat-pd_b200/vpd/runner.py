@@ -32,7 +32,7 @@ import time
 
 import numpy as np
 
-from .boundary_case import BoundaryCase, load_boundary_case
+from .boundary_case import BoundaryCase, indicator_values, load_boundary_case
 from .case import DIAG
 
 TIMESERIES_HEADER = (
@@ -73,17 +73,17 @@ def timeseries_line(label: str, row) -> str:
 
 
 def snapshot_lines(label: str, step: int, time_ms: float, x0, u, v, strain_axial, stress_axial,
-                   eqps, damage) -> str:
-    """field_snapshots.csv lines of every point at one step (internal indicator 0: the
-    Johnson-Cook material has none)."""
+                   eqps, damage, indicator=None) -> str:
+    """field_snapshots.csv lines of every point at one step (``indicator``: the internal
+    indicator per point, 0 when the material configures none)."""
     out = []
     t = g16(time_ms)
     for i in range(len(x0)):
         x = x0[i] + u[i]
         out.append(",".join([label, str(step), t, str(i)] + [g16(a) for a in x0[i]] + [g16(a) for a in u[i]]
                             + [g16(a) for a in x] + [g16(a) for a in v[i]]
-                            + [g16(strain_axial[i]), g16(stress_axial[i]), g16(eqps[i]), "0",
-                               g16(damage[i])]) + "\n")
+                            + [g16(strain_axial[i]), g16(stress_axial[i]), g16(eqps[i]),
+                               "0" if indicator is None else g16(indicator[i]), g16(damage[i])]) + "\n")
     return "".join(out)
 
 
@@ -249,6 +249,8 @@ def run_boundary_case(path: str, out_dir: str = None, config_root: str = None, p
                                        symbol=p.symbol)
                 if m.initial_state:
                     sim.set_initial_state(m.initial_state)
+                if m.indicator is not None:
+                    sim.set_internal_indicator(*m.indicator)
                 if surrogate is not None:
                     w, b = networks.get(case.props, (None, None))
                     sim.set_surrogate(w, b, guess=surrogate, newton_steps=2)
@@ -264,7 +266,8 @@ def run_boundary_case(path: str, out_dir: str = None, config_root: str = None, p
                                             sim.field("displacement"), sim.field("velocity"),
                                             sim.field("strain")[:, 4 * axis],
                                             sim.field("stress_spatial")[:, 4 * axis], eqps,
-                                            sim.field("damage_index")[:, 0]))
+                                            sim.field("damage_index")[:, 0],
+                                            None if m.indicator is None else indicator_values(m.indicator, state)))
             runtime = time.perf_counter() - started
             rows = np.concatenate(chunks)
             if m.eqps_index < 0:  # no eqps variable: the reference reports 0 (:259-261)
