@@ -35,6 +35,11 @@
  *   vpd_set_host_vumat       VumatMaterialAdapter (src/material/VumatMaterialAdapter.cpp:238-362)
  *                            driving any user VUMAT plugin on 256-row blocks, with the rest
  *                            of the increment on the GPU
+ *   vpd_set_initial_state    a material's initialState in VumatPdCorrespondenceMaterial::initialize
+ *                            (VumatPdCorrespondenceMaterial.cpp:62-66, src/config/DemoConfig.cpp:220-251)
+ *   vpd_set_internal_indicator  the internalIndicator of the step diagnostics
+ *                            (BoundaryValueCaseRunner.cpp:93-107, :258-263)
+ *   vpd_checkpoint_*         no counterpart: the state an increment carries, saved and restored
  *   vumat_adapter_call       the plugin entry the reference dlopens
  *                            (materials/bridge/vumat_c_wrapper_jinfo.f90:1-17,
  *                             include/VumatMaterialAdapter.hpp:35-39), Johnson-Cook on the GPU
