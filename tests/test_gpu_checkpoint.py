@@ -11,7 +11,7 @@ import vpd
 from vpd.case import (DAMAGE_CRITICAL_STRETCH, DAMAGE_EQPS_THRESHOLD, MATERIAL_SURROGATE,
                       PRECISION_MIXED, pd_coarse, tensile_bar)
 
-pytestmark = [pytest.mark.gpu, pytest.mark.late]
+pytestmark = pytest.mark.gpu
 
 FIELDS = ("displacement", "velocity", "acceleration", "stress_corotational", "state",
           "damage_index", "temperature")

@@ -21,7 +21,7 @@ from conftest import golden
 import oracle as O
 from vpd.demo_runner import run_demo_case
 
-pytestmark = [pytest.mark.gpu, pytest.mark.late]
+pytestmark = pytest.mark.gpu
 
 NOISE = {"max_f_error": 1e-12, "net_force_x": 1e-7, "net_force_y": 1e-7, "net_force_z": 1e-7,
          "net_force_norm": 1e-7}

@@ -18,7 +18,7 @@ from conftest import golden
 
 from vpd.point_runner import run_material_point_case
 
-pytestmark = [pytest.mark.gpu, pytest.mark.late]
+pytestmark = pytest.mark.gpu
 
 
 def test_stock_jc_material_point_on_gpu(tmp_path):

@@ -23,7 +23,7 @@ from conftest import golden
 import oracle as O
 from vpd.runner import run_boundary_case
 
-pytestmark = [pytest.mark.gpu, pytest.mark.late, pytest.mark.skipif(
+pytestmark = [pytest.mark.gpu, pytest.mark.skipif(
     not os.path.exists(os.path.join(O.REF_DIR, "vumat_pd_run")), reason="reference CLI not built")]
 CLI = os.path.join(O.REF_DIR, "vumat_pd_run")
 
