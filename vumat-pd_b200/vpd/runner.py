@@ -299,7 +299,9 @@ def main(argv=None) -> int:
     ap.add_argument("--plugin-dir", help="directory of the materials' VUMAT plugins (default: the "
                     "stock Johnson-Cook plugin is this package's GPU library)")
     ap.add_argument("--precision", choices=("fp64", "mixed"), default="fp64",
-                    help="boundary-value cases: FP64 throughout (the drop-in), or FP32 bond sums")
+                    help="boundary-value cases: FP64 throughout (the drop-in), or FP32 bond sums "
+                         "(whose net internal force exceeds the cases' FP64 round-off limit, so "
+                         "the verdict reports fail)")
     ap.add_argument("--surrogate", choices=SURROGATE_GUESSES,
                     help="boundary-value cases: the learned Johnson-Cook return map with this guess "
                          "(the network is trained on the GPU first; the VUMAT stays the fallback)")
