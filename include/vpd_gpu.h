@@ -266,8 +266,10 @@ int vpd_force_density(const double *positions, const double *volumes, int64_t n,
    results and errors as vpd_force_density; its scratch is a fixed array inside the library
    (about 4.7 MB held on each GPU that loads it). At most 65536 points per call, else
    VPD_ERR_CAPACITY. Calls share the scratch: calls that overlap on the GPU race. The first
-   call on a device looks up the scratch address; make it before any stream capture.
-   Synchronises the stream. (No counterpart in the reference.) */
+   call on a device looks up the scratch address, which (CUDA loads modules lazily) loads the
+   library's code for this entry point and with it reserves the 4.7 MB scratch on that
+   device: make that first call before the host's pool takes the device memory and before
+   any stream capture. Synchronises the stream. (No counterpart in the reference.) */
 int vpd_force_density_noalloc(const double *positions, const double *volumes, int64_t n,
                               const int64_t *row_ptr, const int32_t *col, const double *kinv,
                               const double *defgrad, const double *cauchy_stress,

@@ -17,7 +17,9 @@ def pytest_configure(config):
 
 
 def pytest_collection_modifyitems(session, config, items):
-    items.sort(key=lambda item: item.get_closest_marker("late") is not None)  # stable
+    # stable: `late` tests after the others, and the no-allocation entry point's file last of all
+    items.sort(key=lambda item: (os.path.basename(str(item.fspath)) == "test_zz_no_alloc.py",
+                                 item.get_closest_marker("late") is not None))
 
 
 def golden(name):
@@ -43,6 +45,18 @@ def load_golden_timeseries():
     with gzip.open(golden("pd_coarse_timeseries.csv.gz"), "rt") as f:
         rows = list(csv.reader(f))
     return rows[0][1:], np.array([[float(x) for x in r[1:]] for r in rows[1:]])
+
+
+def build_abi_host(out_dir):
+    """Compiles tests/abi_host.cpp (the C++ host on include/vpd_gpu.h) against the in-tree
+    libvpd_gpu.so with the system compiler; returns the executable's path."""
+    import subprocess
+    lib_dir = os.path.join(ROOT, "vumat-pd_b200")
+    exe = os.path.join(str(out_dir), "abi_host")
+    subprocess.run(["g++", "-std=c++17", "-O2", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "abi_host.cpp"), "-o", exe,
+                    os.path.join(lib_dir, "libvpd_gpu.so"), f"-Wl,-rpath,{lib_dir}"], check=True)
+    return exe
 
 
 @pytest.fixture(scope="session")

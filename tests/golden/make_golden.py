@@ -2,7 +2,7 @@
 
 Run here (where the reference sources are mounted) after `make -C oracle`:
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py REFERENCE_CHECKOUT [--cases-only | --examples]
 
 Fixtures (read by the tests; nothing at test time reads the reference checkout):
   pd_coarse_timeseries.csv.gz  the reference's archived JC run
@@ -30,8 +30,23 @@ Fixtures (read by the tests; nothing at test time reads the reference checkout):
                                sources by oracle/Makefile, plugins the restated JC and elastic
                                routines) run on each example case: its output files, gzipped
 
+  ref_config3_slab.npz         the reference library on a 24-plane slab of the jittered 1M-point
+                               steel bar (24x50x50 points, horizon 4.015 h, +-0.05 h jitter,
+                               workToHeat 1e6, grips at 5 m/s, critical stretch 0.02), FP64:
+                               160 timeseries rows, the final damage index of every point, and
+                               the final displacement, corotational stress and state (eqps,
+                               iteration count) of every 13th point
+  archived_pd_cases.npz        for each archived PD case (raw/pd_*): its timeseries, its final
+                               displacement interpolated at the analysis script's 1551 sample
+                               coordinates (analyse_and_plot.py:46-66), and the archived FEM
+                               reference (raw/fem_reference) as those metrics read it: its axial
+                               stress at the 240 common output times, its final displacement at
+                               the sample coordinates, its last stress and max eqps
+  expected_pd_metrics.json     the PD rows of benchmarks/tensile3d/expected/analysis.json
+
 `--cases-only` refreshes only cases/, configs/ and the snapshot head; `--examples` only the
-example cases and their outputs.
+example cases and their outputs; `--config3` only ref_config3_slab.npz; `--archived` only the
+archived PD case fixtures.
 """
 import csv
 import gzip
@@ -96,6 +111,64 @@ def run_examples(reference):
         shutil.rmtree(scratch)
 
 
+CONFIG3_SLAB_STEPS = 160
+CONFIG3_SLAB_STRIDE = 13
+
+
+def config3_slab():
+    """The reference library (compiled into oracle/_ref) on a slab of the config-3 bar."""
+    import oracle as O
+    from vpd.case import tensile_bar
+    case = tensile_bar(3, nx=24, precision=0)
+    sim = O.RefSim(case)
+    diag = sim.step(CONFIG3_SLAB_STEPS)
+    pick = np.arange(0, sim.n_points, CONFIG3_SLAB_STRIDE)
+    sigma = sim.get("stress_corotational")[pick][:, [0, 4, 8, 1, 5, 2]]
+    np.savez_compressed(os.path.join(HERE, "ref_config3_slab.npz"), diag=diag,
+                        damage_index=sim.get("damage_index")[:, 0],
+                        stride=CONFIG3_SLAB_STRIDE,
+                        displacement=sim.get("displacement")[pick],
+                        stress_corotational6=sigma, state=sim.get("state")[pick][:, [1, 5]])
+    sim.close()
+
+
+def archived_cases(reference):
+    """The archived PD runs and the FEM reference, reduced to what the analysis metrics read."""
+    sys.path.insert(0, os.path.join(ROOT, "vumat-pd_b200"))
+    from vpd.metrics import COMMON_TIMES, interpolate_nodes, read_csv, sample_coordinates
+    import json
+    raw = os.path.join(reference, "benchmarks", "tensile3d", "raw")
+    coords = sample_coordinates()
+    out = {}
+    fem_ts = read_csv(os.path.join(raw, "fem_reference", "timeseries.csv.gz"))
+    fem_nodes = read_csv(os.path.join(raw, "fem_reference", "final_nodes.csv.gz"))
+    out["fem_reference_stress"] = np.interp(COMMON_TIMES, fem_ts["time_ms"],
+                                            fem_ts["average_axial_stress_MPa"])
+    out["fem_reference_final_stress"] = fem_ts["average_axial_stress_MPa"][-1]
+    out["fem_reference_max_eqps"] = fem_ts["max_eqps"][-1]
+    out["fem_reference_u"] = interpolate_nodes(fem_nodes, coords)
+    names = sorted(n for n in os.listdir(raw) if n.startswith("pd_"))
+    for name in names:
+        ts = read_csv(os.path.join(raw, name, "timeseries.csv.gz"))
+        cols = [k for k in ts]
+        out[f"{name}_timeseries"] = np.stack([ts[k] for k in cols], 1)
+        out[f"{name}_columns"] = np.array(cols)
+        snap = read_csv(os.path.join(raw, name, "field_snapshots.csv.gz"))
+        out[f"{name}_u"] = interpolate_nodes(snap, coords)
+        with open(os.path.join(raw, name, "metadata.json")) as f:
+            meta = json.load(f)
+        m = meta["materials"][0]
+        out[f"{name}_summary"] = np.array([m["maxEqps"], m["finalReaction_N"],
+                                           m["finalEnergyError"], m["earlyElasticSlope_MPa"]])
+    np.savez_compressed(os.path.join(HERE, "archived_pd_cases.npz"), **out)
+    with open(os.path.join(reference, "benchmarks", "tensile3d", "expected", "analysis.json")) as f:
+        expected = json.load(f)["metrics"]
+    with open(os.path.join(HERE, "expected_pd_metrics.json"), "w") as f:
+        json.dump({k: v for k, v in expected.items() if k.startswith("pd_")}, f, indent=1,
+                  sort_keys=True)
+        f.write("\n")
+
+
 def main(reference):
     copy_cases(reference)
     import oracle as O
@@ -156,16 +229,24 @@ def main(reference):
         for k, v in second.items():
             out[f"{tag}_{k}"] = v
     np.savez_compressed(os.path.join(HERE, "ref_jc_thermal.npz"), **out)
+    config3_slab()
+    archived_cases(reference)
     print("fixtures written to", HERE)
 
 
 if __name__ == "__main__":
     args = [a for a in sys.argv[1:] if not a.startswith("--")]
-    ref = args[0] if args else "/root/reference"
+    if not args or not os.path.isdir(os.path.join(args[0], "src")):
+        sys.exit("usage: make_golden.py REFERENCE_CHECKOUT [--cases-only | --examples]")
+    ref = args[0]
     if "--cases-only" in sys.argv:
         copy_cases(ref)
     elif "--examples" in sys.argv:
         run_examples(ref)
+    elif "--config3" in sys.argv:
+        config3_slab()
+    elif "--archived" in sys.argv:
+        archived_cases(ref)
     else:
         main(ref)
         run_examples(ref)

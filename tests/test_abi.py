@@ -10,7 +10,7 @@ import tempfile
 import numpy as np
 import pytest
 
-from conftest import ROOT
+from conftest import ROOT, build_abi_host
 
 import vpd
 from vpd.case import VpdCase, pd_coarse, stable_dt, tensile_bar
@@ -55,6 +55,16 @@ def test_struct_layouts_match_c(ctype, pytype):
     out = c_layout(ctype, fields)
     assert out[0] == ctypes.sizeof(pytype)
     assert out[1:] == [getattr(pytype, f).offset for f in fields]
+
+
+def test_compiled_cpp_host_sees_the_python_struct_layout(tmp_path):
+    """tests/abi_host.cpp, the C++ host compiled against the header and linked to the library,
+    reports the vpd_case layout the ctypes mirror (vpd.case.VpdCase) assumes."""
+    exe = build_abi_host(tmp_path)
+    out = subprocess.run([exe, "layout"], capture_output=True, text=True, check=True).stdout
+    layout = dict((k, int(v)) for k, v in (line.split() for line in out.splitlines()))
+    assert layout.pop("sizeof") == ctypes.sizeof(VpdCase)
+    assert layout == {f[0]: getattr(VpdCase, f[0]).offset for f in VpdCase._fields_}
 
 
 def test_invalid_cases_rejected_on_host():

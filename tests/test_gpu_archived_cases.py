@@ -1,0 +1,72 @@
+"""Every archived PD case file of the reference's tensile benchmark
+(benchmarks/tensile3d/cases/pd_*.json) run on the GPU through the case-file runner, as
+`vumat_pd_run CASE.json` runs it on the CPU:
+
+  * the timeseries against the archived run's (raw/pd_*/timeseries.csv): stress history NRMSE
+    below 1e-6, the other columns within 1e-7 of their scale;
+  * the final displacement at the analysis script's 1551 sample coordinates against the
+    archived snapshot's, within 1e-8 of its scale;
+  * the summary numbers of metadata.json against the archived ones;
+  * the analysis metrics (vpd.metrics, the PD half of analyse_and_plot.py) against the frozen
+    expected/analysis.json values with verify_metrics.py's 0.5 % tolerance.
+"""
+import json
+import math
+
+import numpy as np
+import pytest
+
+from conftest import golden, max_rel, nrmse
+
+from vpd import metrics as VM
+
+pytestmark = pytest.mark.gpu
+
+CASES = ("pd_coarse", "pd_delta2", "pd_delta4", "pd_dt12p5", "pd_dt50", "pd_m1p5", "pd_shared")
+
+
+@pytest.fixture(scope="module")
+def archive():
+    data = np.load(golden("archived_pd_cases.npz"))
+    with open(golden("expected_pd_metrics.json")) as f:
+        expected = json.load(f)
+    ref = {"stress": data["fem_reference_stress"], "u": data["fem_reference_u"],
+           "final_stress": float(data["fem_reference_final_stress"]),
+           "max_eqps": float(data["fem_reference_max_eqps"])}
+    return data, expected, ref
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_archived_case_runs_on_the_gpu(archive, name, tmp_path):
+    from vpd.runner import run_boundary_case
+    data, expected, ref = archive
+    rc = run_boundary_case(golden(f"cases/{name}.json"), str(tmp_path), golden(""), log=lambda line: None)
+    assert rc == 0  # the reference's acceptance verdict, as archived: pass
+    mine = VM.read_csv(str(tmp_path / "timeseries.csv"))
+    cols = [str(c) for c in data[f"{name}_columns"]]
+    arch = {c: data[f"{name}_timeseries"][:, j] for j, c in enumerate(cols)}
+    assert np.array_equal(mine["step"], arch["step"])
+    assert nrmse(mine["average_axial_stress_MPa"], arch["average_axial_stress_MPa"]) < 1e-6
+    for c in ("reaction_force_N", "max_eqps", "kinetic_energy_Nmm", "internal_energy_Nmm",
+              "external_work_Nmm", "lateral_strain", "average_axial_strain", "load_displacement_mm"):
+        assert max_rel(mine[c], arch[c]) < 1e-7, c
+    assert np.all(mine["finite"] == 1.0)
+
+    snap = VM.read_csv(str(tmp_path / "field_snapshots.csv"))
+    u = VM.interpolate_nodes(snap, VM.sample_coordinates())
+    assert max_rel(u, data[f"{name}_u"]) < 1e-8
+
+    with open(tmp_path / "metadata.json") as f:
+        meta = json.load(f)
+    m = meta["materials"][0]
+    max_eqps, reaction, energy_error, slope = data[f"{name}_summary"]
+    assert meta["status"] == "pass" and m["status"] == "pass"
+    assert m["maxEqps"] == pytest.approx(max_eqps, rel=1e-7)
+    assert m["finalReaction_N"] == pytest.approx(reaction, rel=1e-7)
+    assert m["finalEnergyError"] == pytest.approx(energy_error, rel=1e-6)
+    assert m["earlyElasticSlope_MPa"] == pytest.approx(slope, rel=1e-7)
+
+    got = VM.run_metrics(str(tmp_path), ref)
+    assert VM.mismatches(expected[name], got) == [], (got, expected[name])
+    for k in ("stress_history_pct", "displacement_pct", "max_eqps_pct", "final_stress_pct"):
+        assert math.isclose(got[k], expected[name][k], rel_tol=1e-5, abs_tol=1e-9), k

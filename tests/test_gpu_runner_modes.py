@@ -19,7 +19,7 @@ from conftest import golden, nrmse
 
 from vpd.runner import main
 
-pytestmark = [pytest.mark.gpu, pytest.mark.late]
+pytestmark = pytest.mark.gpu
 
 
 def test_case_file_on_the_surrogate_mixed_path(tmp_path):

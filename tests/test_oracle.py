@@ -202,3 +202,38 @@ def test_reference_interface_contract_with_restated_probe():
     r = subprocess.run([exe, os.path.join(O.REF_DIR, "contract_probe_plugin.so")],
                        capture_output=True, text=True, timeout=120)
     assert r.returncode == 0, r.stdout + r.stderr
+
+
+@pytest.mark.skipif(not O.reference_available(), reason="reference library not built")
+def test_reference_library_config3_slab_cascades():
+    """The reference library itself on a 24-plane slab of the 1M-point benchmark bar (24x50x50,
+    horizon 4.015 h, +-0.05 h jitter, workToHeat 1e6, grips at 5 m/s, critical stretch 0.02):
+    it reproduces the committed fixture the GPU tests compare against, its first bonds break
+    between increments 75 and 100 (before the bar yields, near increment 140), and the failure
+    then cascades -- by increment 225 a fifth of all bonds are broken, nearly every point has
+    lost bonds and the axial stress has fallen to under a third of its peak -- because the
+    correspondence deformation gradient keeps summing over the broken bonds
+    (PdCorrespondenceSkeleton.cpp:172-197 reads no bond damage)."""
+    ref = np.load(golden("ref_config3_slab.npz"))
+    case = tensile_bar(3, nx=24, precision=0)
+    sim = O.RefSim(case)
+    stress = vpd_diag("average_axial_stress_MPa")
+    rows = [sim.step(75)]
+    assert sim.get("damage_index").max() == 0.0
+    rows.append(sim.step(25))
+    assert sim.get("damage_index").max() > 0.0
+    rows.append(sim.step(60))
+    diag = np.concatenate(rows)
+    assert np.array_equal(diag, ref["diag"])  # the fixture is this library's run
+    assert np.array_equal(sim.get("damage_index")[:, 0], ref["damage_index"])
+    more = sim.step(65)
+    d = sim.get("damage_index")[:, 0]
+    assert d.mean() > 0.2 and np.mean(d > 0) > 0.9
+    peak = np.max(np.concatenate([diag[:, stress], more[:, stress]]))
+    assert peak > 350.0 and more[-1, stress] < peak / 3
+    assert more[-1, vpd_diag("max_eqps")] > 0.02
+
+
+def vpd_diag(name):
+    import vpd
+    return vpd.DIAG[name]

@@ -18,8 +18,12 @@
 //     that overlap on the GPU -- on different streams or from different host threads without
 //     ordering between them -- race on it;
 //   * the first call on a device looks up the array's device address (cudaGetSymbolAddress)
-//     with that device current and caches it; make that first call before any stream
-//     capture.
+//     with that device current and caches it. With CUDA's lazy module loading (the default
+//     since CUDA 12.2) that lookup is also what loads this file's device code on the device,
+//     and loading it reserves the 4.7 MB array in device memory at that moment. So the first
+//     call on each device must come before the host hands its device memory to its own pool
+//     (or the load fails with cudaErrorMemoryAllocation, returned as VPD_ERR_CUDA) and before
+//     any stream capture. Later calls reserve nothing.
 #include "vpd_internal.h"
 
 #include <mutex>
