@@ -75,6 +75,8 @@ def parse_args():
     p.add_argument("--train-samples", type=int, default=2_000_000)
     p.add_argument("--train-epochs", type=int, default=20)
     p.add_argument("--no-ablations", action="store_true", help="skip the guess ablations")
+    p.add_argument("--no-config2", action="store_true",
+                   help="skip the 500k-point damaged bar's mixed-against-FP64 record")
     return p.parse_args()
 
 
@@ -292,6 +294,39 @@ def run_reference(args, world, rank):
     }), flush=True)
 
 
+def config2_record(vpd, np, nrmse):
+    """The 200x50x50 bar (500k points, horizon 3.015 h, grips at 1 m/s, critical stretch 0.02)
+    over its full 5000 increments in mixed precision and in plain FP64 (the GPU oracle):
+    particle-steps/s of each, the errors of the mixed run against FP64 (stress history,
+    final displacement and eqps) and the broken bonds of both."""
+    from vpd.case import PRECISION_FP64, PRECISION_MIXED, tensile_bar
+    case = tensile_bar(2)
+    out = {"workload": "tensile_bar_2: 200x50x50 steel JC bar, horizon 3.015 h, grips 1 m/s, "
+                       f"critical stretch 0.02, {case.steps} increments from rest"}
+    runs = {}
+    for name, prec in (("plain_fp64", PRECISION_FP64), ("mixed", PRECISION_MIXED)):
+        with vpd.Simulation(case.replace(precision=prec)) as sim:
+            row_ptr, _ = sim.neighbors()
+            rows = sim.step(case.steps, diagnostics=True)
+            ms = sim.last_step_ms()
+            d = sim.field("damage_index")[:, 0]
+            runs[name] = {"rows": rows, "u": sim.field("displacement"), "eqps": sim.field("state")[:, 1],
+                          "d": d, "broken": float(np.sum(d * np.diff(row_ptr))), "ms": ms,
+                          "n": sim.n_points}
+    ref, mix = runs["plain_fp64"], runs["mixed"]
+    col = vpd.DIAG["average_axial_stress_MPa"]
+    for name, r in runs.items():
+        out[name] = {"value": r["n"] * case.steps / (r["ms"] * 1e-3), "ms_per_step": r["ms"] / case.steps,
+                     "broken_bonds": r["broken"], "max_eqps": float(r["rows"][-1, vpd.DIAG["max_eqps"]]),
+                     "finite": bool(r["rows"][-1, vpd.DIAG["finite"]] == 1.0)}
+    out["stress_nrmse"] = nrmse(mix["rows"][:, col], ref["rows"][:, col])
+    out["displacement_nrmse"] = nrmse(mix["u"], ref["u"])
+    out["eqps_nrmse"] = nrmse(mix["eqps"], ref["eqps"])
+    out["damage_index_equal_fraction"] = float(np.mean(mix["d"] == ref["d"]))
+    out["broken_bond_difference"] = mix["broken"] - ref["broken"]
+    return out
+
+
 def run_gpu(args, world, rank, local):
     import numpy as np
     import torch
@@ -361,6 +396,7 @@ def run_gpu(args, world, rank, local):
     damaged = {"plain_fp64": run(bar.replace(precision=PRECISION_FP64), preload=0),
                "surrogate_mixed": run(bar.replace(precision=PRECISION_MIXED,
                                                   material_mode=MATERIAL_SURROGATE), "hybrid", preload=0)}
+    config2 = None if args.no_config2 else config2_record(vpd, np, nrmse)
     clock = clocks.stop()
     for group in (modes, damaged):
         base = group["plain_fp64"]
@@ -440,6 +476,7 @@ def run_gpu(args, world, rank, local):
         "speedup_vs_plain_fp64": head["value"] / ref["value"],
         "modes": modes,
         "from_rest_with_damage": damaged,
+        "config2_mixed_vs_fp64": config2,
         "surrogate_training": {"final_epoch_loss": report["epoch_loss"][-1],
                                **{k: v for k, v in report.items() if k != "epoch_loss"}},
         "roofline": {"kernel": dominant, "bound": "hbm", "achieved": achieved, "peak": peak,

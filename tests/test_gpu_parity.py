@@ -255,14 +255,18 @@ def test_sliced_ell_layout_matches_stencil_layout(monkeypatch):
         assert np.array_equal(b.field("damage_index"), da)
 
 
-@pytest.mark.parametrize("kind", ["", "tiled2"])
+@pytest.mark.parametrize("dims", [(24, 21, 17), (12, 37, 70)])
+@pytest.mark.parametrize("kind", ["", "tiled4", "tiled2"])
 @pytest.mark.parametrize("damage", [0, 1])
-def test_tiled_fp64_bond_kernels_match_slot_kernels_bitwise(monkeypatch, damage, kind):
-    """The tiled FP64 bond kernels (two points per thread along y; four in the force kernel
-    unless tiled2) sum every point's bonds in the per-slot kernels' order with the same
-    operations: on the jittered horizon-4 bar (y extent 21, so the last tile of a column is
-    ragged) the increments agree bit for bit, bond breaking included."""
-    case = tensile_bar(3, nx=24, ny=21, nz=17, damage_mode=damage, damage_initiation=0.004,
+def test_tiled_fp64_bond_kernels_match_slot_kernels_bitwise(monkeypatch, damage, kind, dims):
+    """The tiled FP64 bond kernels (two points per thread along y; in the force kernel four,
+    from shared memory filled plane by plane by TMA by default, from L1 with tiled4, two with
+    tiled2) sum every point's bonds in the per-slot kernels' order with the same operations:
+    on the jittered horizon-4 bar (y extent 21 and z extent 17, so the last tiles are ragged)
+    the increments agree bit for bit, bond breaking included. The second lattice (z extent 70)
+    takes three staged tiles along z and three along y, the last of each ragged."""
+    nx, ny, nz = dims
+    case = tensile_bar(3, nx=nx, ny=ny, nz=nz, damage_mode=damage, damage_initiation=0.004,
                        precision=PRECISION_FP64)
     fields = ("displacement", "velocity", "stress_corotational", "state", "damage_index")
     monkeypatch.setenv("VPD_BOND_KERNEL", "slot")

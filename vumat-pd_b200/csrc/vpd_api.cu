@@ -303,6 +303,8 @@ int read_status(vpd_handle *h) {
     return set_error(VPD_ERR_SINGULAR, "Corotational update encountered a singular tensor.");
   if (st & STATUS_SURROGATE_WAIT)
     return set_error(VPD_ERR_CUDA, "surrogate material kernel: tensor-core wait timed out");
+  if (st & STATUS_STAGED_WAIT)
+    return set_error(VPD_ERR_CUDA, "staged force kernel: TMA wait timed out");
   return VPD_OK;
 }
 
@@ -439,14 +441,23 @@ int create_impl(vpd_handle *h, const vpd_case *c, const double *positions, const
   p.lat_nx = c->nx, p.lat_ny = c->ny, p.lat_nz = c->nz, p.lat_h = c->spacing;
   {
     // VPD_BOND_KERNEL=slot selects the per-slot bond kernels (both precisions), scalar the
-    // two-point tiled mixed kernels in scalar FP32, tiled2 the two-point FP64 force kernel
-    // (default: tiled, packed pairs when mixed, four points per thread in the FP64 force)
+    // two-point tiled mixed kernels in scalar FP32, pair the packed-pair mixed kernels, tiled2
+    // and tiled4 the unstaged two- and four-point FP64 force kernels (default: tiled; when
+    // mixed the shared-window deformation kernel without damage and packed pairs otherwise;
+    // the TMA-staged FP64 force kernel)
     const char *bk = getenv("VPD_BOND_KERNEL");
     const std::string kind = bk ? bk : "";
-    p.tiled = kind == "slot" ? 0 : (kind == "scalar" ? 1 : (kind == "tiled2" ? 3 : 2));
+    p.tiled = kind == "slot" ? 0
+              : kind == "scalar" ? 1
+              : kind == "tiled2" ? 3
+              : kind == "pair"   ? 4
+              : kind == "tiled4" ? 5
+                                 : 2;
   }
   if (p.st.nw && ((rc = dalloc(h, &p.vxi, n)) ||
                   (c->precision != VPD_PRECISION_MIXED && (rc = dalloc(h, &p.fmap, 3 * n)))))
+    return rc;
+  if (p.st.nw && p.fmap && p.tiled == 2 && (rc = setup_staged_force64(p, p.st.rx, p.st.ry, p.st.rz)))
     return rc;
   p.nstatev = c->nstatev;
   p.flags = h->flags, p.obsw = h->obsw;

@@ -27,6 +27,7 @@ enum : unsigned int {
   STATUS_SINGULAR_F = 2u,
   STATUS_SINGULAR_KINEMATICS = 4u,
   STATUS_SURROGATE_WAIT = 8u,  // a tensor-core wait of the surrogate material kernel timed out
+  STATUS_STAGED_WAIT = 16u,    // a TMA wait of the staged FP64 force kernel timed out
 };
 
 // ---- point flags ----

@@ -204,6 +204,7 @@ int build_stencil(const int64_t *row_ptr, const int32_t *col, int64_t n, int ny,
   st.ngroups = (int)groups.size();
   // a two-point tile's window reaches y in [-ry, ny + ry], x and z within the extent
   st.halo = (int64_t)ex.rx * ny * nz + (int64_t)(ex.ry + 2) * nz + ex.rz + 1;
+  st.rx = ex.rx, st.ry = ex.ry, st.rz = ex.rz;
   return VPD_OK;
 }
 

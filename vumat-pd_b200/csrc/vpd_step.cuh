@@ -3,6 +3,8 @@
 
 #include "vpd_internal.h"
 
+#include <cuda.h>  // CUtensorMap (the staged FP64 force kernel's tensor map)
+
 namespace vpd {
 
 struct BcParams {
@@ -26,6 +28,17 @@ constexpr int kGroupBlocks = 256;   // k_integrate blocks reduced together by th
 constexpr int kBondThreads = 256;    // threads per block of the bond kernels
 constexpr int kMaterialThreads = 128;
 constexpr int kMaxStencilWords = 32; // at most 1024 lattice offsets per stencil
+constexpr int kStagedThreads = 128;  // threads per block of the TMA-staged FP64 force kernel
+constexpr size_t kStagedMaxBytes = 110 * 1024;  // its box, so that two blocks fit an SM
+
+// Tiles of the TMA-staged FP64 force kernel (vpd_staged64.cu); bytes == 0: not in use.
+struct StagedTiles {
+  int tz = 0, ty = 0, qy = 0;          // tile extent along z and y; four-point y columns
+  int ry = 0, rz = 0;                  // the stencil's reach along y and z
+  int by = 0, bz = 0;                  // box extent: tile plus reach on both sides
+  int tiles_y = 0, tiles_z = 0, threads = 0;
+  uint32_t bytes = 0;                  // box bytes: 3 rows x by x bz x 32
+};
 
 // Lattice-stencil bond layout (vpd_stencil.cu). nw == 0: not in use.
 struct StencilLayout {
@@ -38,6 +51,7 @@ struct StencilLayout {
   uint32_t *broken = nullptr;  // [nw][n] broken-bond bits
   float4 *e0 = nullptr;        // [32 nw] lattice offset of each slot times h (mixed precision)
   int64_t halo = 0;            // points a tile's window can reach beyond either end of the lattice
+  int rx = 0, ry = 0, rz = 0;  // the largest |offset| along x, y, z
 };
 
 struct StepParams {
@@ -52,8 +66,9 @@ struct StepParams {
   StencilLayout st;           // lattice-stencil layout; used instead of the ELL when st.nw > 0
   int lat_nx, lat_ny, lat_nz; // the lattice (points in index order (x ny + y) nz + z)
   double lat_h;               // lattice spacing
-  int tiled;                  // bond kernels: 0 per slot; mixed 1 tiled scalar, else packed pairs; FP64 tiled (3: 2-point force)
-                              // (2 or 3), 0 for the per-slot kernels
+  int tiled;                  // bond kernels: 0 per slot; mixed 1 tiled scalar, 4 packed pairs, 2 shared
+                              // windows (packed pairs with damage); FP64 2 tiled with the TMA-staged
+                              // force, 3 tiled with the 2-point force, 5 tiled with the 4-point force
   // kinematic state
   double4 *u0, *u1;           // displacement ping-pong: increment s reads u[s & 1]
   double4 *vel, *acc, *force;
@@ -65,6 +80,8 @@ struct StepParams {
   // fmap[r * n + i] = (VM_r0, VM_r1, VM_r2, X_r), so one bond reads three 32-byte records
   double4 *fmap;
   double4 *vxi;               // sum over all bonds of V_j xi (FP64, set once; stencil layout)
+  StagedTiles staged;         // the TMA-staged FP64 force kernel's tiles and box
+  CUtensorMap fmap_tmap;      // ... and its tensor map over fmap (lane, z, y, x, row)
   // mixed precision (VPD_PRECISION_MIXED): FP32 copies gathered by the bond kernels
   int mixed;
   // mixed precision: jit, uf and fmapf carry st.halo zero records before and after their n
@@ -147,11 +164,17 @@ int launch_deformation_mixed(const StepParams &p, cudaStream_t s);
 int launch_force_mixed(const StepParams &p, cudaStream_t s);
 int launch_mixed_setup(const StepParams &p, int ny, int nz, double h, double yoff, double zoff,
                        cudaStream_t s);
-// tiled mixed-precision bond kernels (vpd_tiled.cu)
+// tiled mixed-precision bond kernels (vpd_tiled.cu; the shared-window deformation kernel in
+// vpd_window.cu)
 int launch_deformation_tiled(const StepParams &p, cudaStream_t s);
+int launch_deformation_window(const StepParams &p, cudaStream_t s);
 int launch_force_tiled(const StepParams &p, cudaStream_t s);
 // tiled FP64 bond kernels (vpd_tiled64.cu)
 int launch_deformation_tiled64(const StepParams &p, cudaStream_t s);
 int launch_force_tiled64(const StepParams &p, cudaStream_t s);
+// TMA-staged FP64 force kernel (vpd_staged64.cu): setup fills p.staged and p.fmap_tmap (left
+// unused when the box does not fit or the driver lacks tensor maps)
+int setup_staged_force64(StepParams &p, int rx, int ry, int rz);
+int launch_force_staged64(const StepParams &p, cudaStream_t s);
 
 }  // namespace vpd
