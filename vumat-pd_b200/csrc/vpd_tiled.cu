@@ -17,8 +17,9 @@
 // body in a runtime loop with 64-bit indices.
 //
 // Arithmetic is that of vpd_mixed.cu: FP32 bond terms, per-group partial sums (folded with
-// Kahan compensation into the force), the FP32 stretch test with a 1e-5 margin and the exact
-// FP64 test inside it, pairs broken once by the lower-index point.
+// Kahan compensation into the force, and in the packed-pair kernels into the deformation sum),
+// the FP32 stretch test with a 1e-5 margin and the exact FP64 test inside it, pairs broken once
+// by the lower-index point.
 #include "vpd_bond.cuh"
 
 namespace vpd {
@@ -432,10 +433,10 @@ __global__ void __launch_bounds__(kBondThreads, 2) k_deformation_pair(const __gr
   pt.jz = make_float2(pa[0].z, pa[1].z);
   pt.ux = make_float2(pb[0].x, pb[1].x), pt.uy = make_float2(pb[0].y, pb[1].y);
   pt.uz = make_float2(pb[0].z, pb[1].z);
-  float2 G[9];
+  float2 G[9], Gc[9];  // the sum of the group partials, with Kahan compensation
 #pragma unroll
   for (int c = 0; c < 9; ++c)
-    G[c] = make_float2(0.0f, 0.0f);
+    G[c] = Gc[c] = make_float2(0.0f, 0.0f);
   int word = -1;  // the mask word held in mw (groups come in slot order: several per word)
   uint32_t mw[2] = {0u, 0u};
   for (int g = 0; g < p.st.ngroups; ++g) {
@@ -492,7 +493,7 @@ __global__ void __launch_bounds__(kBondThreads, 2) k_deformation_pair(const __gr
     }
 #pragma unroll
     for (int c = 0; c < 9; ++c)
-      G[c] = __fadd2_rn(G[c], part[c]);
+      kahan_add2(G[c], Gc[c], part[c]);
     if (DAMAGE)
 #pragma unroll
       for (int q = 0; q < 2; ++q)
@@ -500,10 +501,11 @@ __global__ void __launch_bounds__(kBondThreads, 2) k_deformation_pair(const __gr
   }
 #pragma unroll
   for (int c = 0; c < 9; ++c) {
+    const float2 g = sub2(G[c], Gc[c]);
     if (vp[0])
-      p.Gf[c * n + ip[0]] = G[c].x;
+      p.Gf[c * n + ip[0]] = g.x;
     if (vp[1])
-      p.Gf[c * n + ip[1]] = G[c].y;
+      p.Gf[c * n + ip[1]] = g.y;
   }
 }
 
