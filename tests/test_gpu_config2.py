@@ -1,0 +1,55 @@
+"""The 500k-point bar of the second benchmark configuration (200x50x50, h = 0.1 mm, horizon
+3.015 h, grips at 1 m/s, critical stretch 0.02) over its full 5000 increments, mixed precision
+(FP32 bond sums, Kahan-compensated) against the plain FP64 path as the GPU oracle.
+
+The bar yields from about increment 2500; its first bonds break near increment 4450 and the
+failure then runs through the whole bar: by increment 5000 practically every bond is broken in
+both runs, and the stresses of the broken-up bar are meaningless. So the stress history is
+compared up to the onset of failure (tolerance 0.5 %, measured ~3e-8), the onset is compared
+between the runs (within one 50-increment window; counts 100 increments later within 5 %), and the end state is
+compared as a count of broken bonds (within 1e-5 of the FP64 count, measured ~1e-7) and the
+fraction of points whose damage index is identical."""
+import numpy as np
+import pytest
+
+from conftest import nrmse
+
+import vpd
+from vpd.case import PRECISION_FP64, PRECISION_MIXED, tensile_bar
+
+pytestmark = pytest.mark.gpu
+
+STRESS = vpd.DIAG["average_axial_stress_MPa"]
+CHUNK = 50
+
+
+def run(precision):
+    case = tensile_bar(2, precision=precision)
+    rows, broken = [], []
+    with vpd.Simulation(case) as sim:
+        row_ptr, _ = sim.neighbors()
+        nb = np.diff(row_ptr)
+        for _ in range(case.steps // CHUNK):
+            rows.append(sim.step(CHUNK))
+            broken.append(float(np.sum(sim.field("damage_index")[:, 0] * nb)))
+        d = sim.field("damage_index")[:, 0]
+        total = float(nb.sum())
+    return np.concatenate(rows), np.array(broken), d, total
+
+
+def test_config2_mixed_against_fp64_through_failure():
+    r64, b64, d64, total = run(PRECISION_FP64)
+    r32, b32, d32, _ = run(PRECISION_MIXED)
+    assert r64.shape[0] == 5000 and np.all(r64[:, vpd.DIAG["finite"]] == 1.0)
+    first64, first32 = int(np.argmax(b64 > 0)), int(np.argmax(b32 > 0))
+    assert b64[-1] > 0 and first64 > 40  # no bond breaks before increment 2000
+    onset = first64 * CHUNK  # the last increment before the first broken bond (FP64)
+    assert r64[onset - 1, vpd.DIAG["max_eqps"]] > 1e-3  # the bar flows plastically first
+    assert nrmse(r32[:onset, STRESS], r64[:onset, STRESS]) < 5e-3
+    assert nrmse(r32[:onset, STRESS], r64[:onset, STRESS]) < 1e-5  # measured ~3e-8
+    assert abs(first32 - first64) <= 1  # the same 50-increment window, or the next
+    k = first64 + 2
+    assert abs(b32[k] - b64[k]) <= 0.05 * b64[k]
+    assert abs(b32[-1] - b64[-1]) <= 1e-5 * b64[-1]
+    assert b64[-1] > 0.99 * total  # the bar has come apart
+    assert np.mean(d32 == d64) > 0.99

@@ -80,3 +80,29 @@ def test_config3_slab_mixed_paths_against_reference_library(ref, mode):
     pick = np.arange(0, len(f["damage_index"]), int(ref["stride"]))
     u_ref = ref["displacement"]
     assert np.sqrt(np.mean((f["displacement"][pick] - u_ref) ** 2)) / np.abs(u_ref).max() < 5e-3
+
+
+def test_config3_bar_with_damage_comes_apart():
+    """The whole 1M-point bar as specified (critical stretch 0.02), plain FP64: its first bonds
+    break between increments 100 and 200, near the grips and before the bar yields; by
+    increment 800 nine tenths of all bonds are broken and the equivalent plastic strain has run
+    away (the correspondence F keeps summing over broken bonds). Without damage the same bar
+    stays intact and flows plastically (the benchmark's headline workload)."""
+    S = vpd.DIAG
+    case = tensile_bar(3, precision=PRECISION_FP64)
+    first = None
+    with vpd.Simulation(case) as sim:
+        for done in range(25, 801, 25):
+            rows = sim.step(25)
+            d = sim.field("damage_index")[:, 0]
+            if first is None and d.max() > 0:
+                first = done
+                assert rows[-1, S["plastic_points"]] == 0  # breaks before anything yields
+        assert 100 < first <= 200
+        assert d.mean() > 0.9 and np.mean(d > 0) > 0.999
+        assert rows[-1, S["max_eqps"]] > 1.0
+    with vpd.Simulation(case.replace(damage_mode=0)) as sim:
+        rows = sim.step(800)
+        assert np.all(rows[:, S["finite"]] == 1.0)
+        assert 0 < rows[-1, S["max_eqps"]] < 0.05
+        assert rows[-1, S["plastic_points"]] > 1000

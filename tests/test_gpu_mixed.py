@@ -65,12 +65,11 @@ def test_thin_lattice_windows_reach_past_both_ends(monkeypatch):
     case = tensile_bar(3, nx=8, ny=3, nz=5, damage_mode=0, precision=PRECISION_MIXED)
     monkeypatch.setenv("VPD_BOND_KERNEL", "slot")
     rs, us, _, _ = run(case, 300)
-    for kind in ("pair", "default"):
-        monkeypatch.setenv("VPD_BOND_KERNEL", kind)
-        rp, up, _, _ = run(case, 300)
-        assert np.all(np.isfinite(rp)) and np.all(np.isfinite(up))
-        assert nrmse(rp[:, STRESS], rs[:, STRESS]) < 1e-5
-        assert nrmse(up, us) < 1e-5
+    monkeypatch.setenv("VPD_BOND_KERNEL", "pair")
+    rp, up, _, _ = run(case, 300)
+    assert np.all(np.isfinite(rp)) and np.all(np.isfinite(up))
+    assert nrmse(rp[:, STRESS], rs[:, STRESS]) < 1e-5
+    assert nrmse(up, us) < 1e-5
     monkeypatch.delenv("VPD_BOND_KERNEL")
     r64, u64, _, _ = run(case.replace(precision=PRECISION_FP64), 300)
     assert nrmse(rp[:, STRESS], r64[:, STRESS]) < 1e-4
@@ -87,8 +86,7 @@ def test_mixed_requires_lattice_layout(monkeypatch):
 @pytest.mark.parametrize("damage", [0, 1])
 def test_tiled_bond_kernels_match_slot_kernels(monkeypatch, damage):
     """The tiled bond kernels (two points per thread along y, one load per neighbour record
-    per stencil group; scalar FP32, packed FP32 pairs, and the default shared-window
-    deformation and full-group force kernels) against the per-slot kernels on the
+    per stencil group; scalar FP32 and packed FP32 pairs) against the per-slot kernels on the
     jittered horizon-4 bar: the same FP32 bond terms summed in another order, so the histories
     agree to FP32 rounding and the bond-breaking decisions agree. With damage the comparison covers the early increments:
     later, rounding-level differences flip bonds at the threshold and the fracture paths part
@@ -98,7 +96,7 @@ def test_tiled_bond_kernels_match_slot_kernels(monkeypatch, damage):
     steps = 120 if damage else 400
     monkeypatch.setenv("VPD_BOND_KERNEL", "slot")
     rs, us, es, ds = run(case, steps)
-    for kind in ("scalar", "pair", "default"):  # default: shared windows / full-group force
+    for kind in ("scalar", "pair"):
         monkeypatch.setenv("VPD_BOND_KERNEL", kind)
         rt, ut, et, dt_ = run(case, steps)
         assert nrmse(rt[:, STRESS], rs[:, STRESS]) < 1e-5

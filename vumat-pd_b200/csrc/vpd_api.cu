@@ -441,10 +441,9 @@ int create_impl(vpd_handle *h, const vpd_case *c, const double *positions, const
   p.lat_nx = c->nx, p.lat_ny = c->ny, p.lat_nz = c->nz, p.lat_h = c->spacing;
   {
     // VPD_BOND_KERNEL=slot selects the per-slot bond kernels (both precisions), scalar the
-    // two-point tiled mixed kernels in scalar FP32, pair the packed-pair mixed kernels, tiled2
-    // and tiled4 the unstaged two- and four-point FP64 force kernels (default: tiled; when
-    // mixed the shared-window deformation kernel without damage and packed pairs otherwise;
-    // the TMA-staged FP64 force kernel)
+    // two-point tiled mixed kernels in scalar FP32, tiled2 and tiled4 the two- and four-point
+    // FP64 force kernels reading through L1 (default: tiled; packed pairs when mixed; the
+    // TMA-staged FP64 force kernel)
     const char *bk = getenv("VPD_BOND_KERNEL");
     const std::string kind = bk ? bk : "";
     p.tiled = kind == "slot" ? 0

@@ -25,6 +25,8 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <cstdlib>
+#include <string>
 
 namespace vpd {
 
@@ -47,19 +49,23 @@ __device__ __forceinline__ void tma_load_5d(void *dst, const CUtensorMap *map, i
       : "memory");
 }
 
-// A 32-byte record of the box, its halves read in the lane's order (see the file comment).
+// A 32-byte record of the box, its halves read in the lane's order (see the file comment);
+// without SWAP in their natural order.
+template <bool SWAP>
 __device__ __forceinline__ double4 lds_record(const double4 *rec, int swap) {
+  if (!SWAP)
+    return *rec;
   const double2 *h = reinterpret_cast<const double2 *>(rec);
   const double2 first = h[swap], second = h[swap ^ 1];
   const double2 lo = swap ? second : first, hi = swap ? first : second;
   return make_double4(lo.x, lo.y, hi.x, hi.y);
 }
 
-template <int P>
+template <int P, bool SWAP>
 __device__ __forceinline__ void staged_element(const double4 *r0, const double4 *r1, const double4 *r2, int swap,
                                                int t, int cnt, const double (&px)[P], const double (&py)[P],
                                                const double (&pz)[P], const uint32_t (&bits)[P], double (&f)[P][3]) {
-  const double4 a = lds_record(r0, swap), c = lds_record(r1, swap), d = lds_record(r2, swap);
+  const double4 a = lds_record<SWAP>(r0, swap), c = lds_record<SWAP>(r1, swap), d = lds_record<SWAP>(r2, swap);
 #pragma unroll
   for (int q = 0; q < P; ++q) {
     if (t < q || t - q >= cnt)
@@ -73,7 +79,7 @@ __device__ __forceinline__ void staged_element(const double4 *r0, const double4 
 }
 
 // The window of one group from the box: record of window position t at box row yy0 + t.
-template <int CNT, int P>
+template <int CNT, int P, bool SWAP>
 __device__ __forceinline__ void staged_window(const double4 *box, int plane, int bz, int cnt, int yy0, int zz,
                                               int swap, const double (&px)[P], const double (&py)[P],
                                               const double (&pz)[P], const uint32_t (&bits)[P], double (&f)[P][3]) {
@@ -81,19 +87,18 @@ __device__ __forceinline__ void staged_window(const double4 *box, int plane, int
 #pragma unroll
     for (int t = 0; t < CNT + P - 1; ++t) {
       const int k = (yy0 + t) * bz + zz;
-      staged_element<P>(box + k, box + plane + k, box + 2 * plane + k, swap, t, CNT, px, py, pz, bits, f);
+      staged_element<P, SWAP>(box + k, box + plane + k, box + 2 * plane + k, swap, t, CNT, px, py, pz, bits, f);
     }
   } else {
     for (int t = 0; t < cnt + P - 1; ++t) {
       const int k = (yy0 + t) * bz + zz;
-      staged_element<P>(box + k, box + plane + k, box + 2 * plane + k, swap, t, cnt, px, py, pz, bits, f);
+      staged_element<P, SWAP>(box + k, box + plane + k, box + 2 * plane + k, swap, t, cnt, px, py, pz, bits, f);
     }
   }
 }
 
-template <bool UNROLL>
-__global__ void __launch_bounds__(kStagedThreads, 2) k_force_staged64(const __grid_constant__ StepParams p) {
-  constexpr int P = 4;
+template <int P, int THREADS, bool SWAP>
+__global__ void __launch_bounds__(THREADS, 2) k_force_staged64(const __grid_constant__ StepParams p) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ __align__(8) uint64_t mbar;
   const double4 *box = reinterpret_cast<const double4 *>(smem);
@@ -106,7 +111,7 @@ __global__ void __launch_bounds__(kStagedThreads, 2) k_force_staged64(const __gr
   const int tyi = b % T.tiles_y, x = b / T.tiles_y;
   const int ty0 = tyi * T.ty, tz0 = tzi * T.tz;
   const int tid = threadIdx.x;
-  // the thread's column: z = tz0 + zl, y = y0 .. y0 + 3; threads past the tile's columns
+  // the thread's column: z = tz0 + zl, y = y0 .. y0 + P - 1; threads past the tile's columns
   // take column 0 (their points are invalid), so every box index stays inside the box
   int zl = tid % T.tz, ql = tid / T.tz;
   const bool active = ql < T.qy;
@@ -181,22 +186,20 @@ __global__ void __launch_bounds__(kStagedThreads, 2) k_force_staged64(const __gr
       if (__all_sync(0xffffffffu, any == 0u))
         continue;
       const int yy0 = (y0 - ty0) + gr.z + T.ry, zz = zl + gr.y + T.rz;
-      if (UNROLL) {
+      {
         static_assert(kUnrolledSlots == 12, "the cases below list the unrolled slot counts");
 #define VPD_STAGED_CASE(C)                                                                  \
   case C:                                                                                   \
-    staged_window<C, P>(box, plane, T.bz, cnt, yy0, zz, swap, px, py, pz, bits, f);          \
+    staged_window<C, P, SWAP>(box, plane, T.bz, cnt, yy0, zz, swap, px, py, pz, bits, f);   \
     break;
         switch (cnt) {
           VPD_STAGED_CASE(1) VPD_STAGED_CASE(2) VPD_STAGED_CASE(3) VPD_STAGED_CASE(4)
           VPD_STAGED_CASE(5) VPD_STAGED_CASE(6) VPD_STAGED_CASE(7) VPD_STAGED_CASE(8)
           VPD_STAGED_CASE(9) VPD_STAGED_CASE(10) VPD_STAGED_CASE(11) VPD_STAGED_CASE(12)
         default:
-          staged_window<0, P>(box, plane, T.bz, cnt, yy0, zz, swap, px, py, pz, bits, f);
+          staged_window<0, P, SWAP>(box, plane, T.bz, cnt, yy0, zz, swap, px, py, pz, bits, f);
         }
 #undef VPD_STAGED_CASE
-      } else {
-        staged_window<0, P>(box, plane, T.bz, cnt, yy0, zz, swap, px, py, pz, bits, f);
       }
     }
     __syncthreads();  // every thread is done with the box before the next plane's copy
@@ -227,8 +230,33 @@ __global__ void __launch_bounds__(kStagedThreads, 2) k_force_staged64(const __gr
 
 }  // namespace
 
+// The kernel's variants: points per thread along y, threads per block, halves read in
+// alternating order (VPD_STAGED: "4x128s" the default, "4x128", "2x256s", "2x256").
+struct StagedVariant {
+  int p, threads;
+  bool swap;
+};
+
+static StagedVariant staged_variant() {
+  const char *v = getenv("VPD_STAGED");
+  const std::string s = v ? v : "";
+  if (s == "4x128")
+    return {4, 128, false};
+  if (s == "2x256s")
+    return {2, 256, true};
+  if (s == "2x256")
+    return {2, 256, false};
+  return {4, 128, true};
+}
+
+template <int P, int THREADS, bool SWAP> static int set_smem(size_t bytes) {
+  VPD_CUDA(cudaFuncSetAttribute(k_force_staged64<P, THREADS, SWAP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)bytes));
+  return VPD_OK;
+}
+
 // Tile shape and tensor map for the staged kernel: tiles span the whole z extent up to 64
-// points (else 32) and as many four-point y columns as fit 128 threads; the box adds the
+// points (else 32) and as many P-point y columns as fit the block's threads; the box adds the
 // stencil's reach on each side. Leaves p.staged.bytes 0 (the tiled kernel runs) when the box
 // would not fit two blocks per SM or the driver entry point is missing.
 int setup_staged_force64(StepParams &p, int rx, int ry, int rz) {
@@ -236,17 +264,19 @@ int setup_staged_force64(StepParams &p, int rx, int ry, int rz) {
   p.staged = StagedTiles{};
   if (!p.fmap || p.st.nw == 0)
     return VPD_OK;
+  const StagedVariant V = staged_variant();
   StagedTiles T{};
+  T.p = V.p, T.swap = V.swap;
   T.tz = p.lat_nz <= 64 ? p.lat_nz : 32;
-  const int cols_y = (p.lat_ny + 3) / 4;
-  T.qy = std::max(1, std::min(kStagedThreads / T.tz, cols_y));
-  T.ty = 4 * T.qy;
+  const int cols_y = (p.lat_ny + V.p - 1) / V.p;
+  T.qy = std::max(1, std::min(V.threads / T.tz, cols_y));
+  T.ty = V.p * T.qy;
   T.ry = ry, T.rz = rz;
   T.by = T.ty + 2 * ry, T.bz = T.tz + 2 * rz;
   T.tiles_y = (p.lat_ny + T.ty - 1) / T.ty;
   T.tiles_z = (p.lat_nz + T.tz - 1) / T.tz;
   const size_t bytes = (size_t)3 * T.by * T.bz * sizeof(double4);
-  if (T.by > 256 || T.bz > 256 || bytes > kStagedMaxBytes || T.qy * T.tz > kStagedThreads)
+  if (T.by > 256 || T.bz > 256 || bytes > kStagedMaxBytes || T.qy * T.tz > V.threads)
     return VPD_OK;
   T.threads = ((T.qy * T.tz + 31) / 32) * 32;
   T.bytes = (uint32_t)bytes;
@@ -270,7 +300,10 @@ int setup_staged_force64(StepParams &p, int rx, int ry, int rz) {
       CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS)
     return set_error(VPD_ERR_CUDA, "cuTensorMapEncodeTiled failed for the force map");
-  VPD_CUDA(cudaFuncSetAttribute(k_force_staged64<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  int rc = V.p == 4 ? (V.swap ? set_smem<4, 128, true>(bytes) : set_smem<4, 128, false>(bytes))
+                    : (V.swap ? set_smem<2, 256, true>(bytes) : set_smem<2, 256, false>(bytes));
+  if (rc)
+    return rc;
   p.staged = T;
   return VPD_OK;
 }
@@ -278,7 +311,12 @@ int setup_staged_force64(StepParams &p, int rx, int ry, int rz) {
 int launch_force_staged64(const StepParams &p, cudaStream_t s) {
   const StagedTiles &T = p.staged;
   const unsigned grid = (unsigned)((int64_t)p.lat_nx * T.tiles_y * T.tiles_z);
-  k_force_staged64<true><<<grid, T.threads, T.bytes, s>>>(p);
+  if (T.p == 4)
+    T.swap ? k_force_staged64<4, 128, true><<<grid, T.threads, T.bytes, s>>>(p)
+           : k_force_staged64<4, 128, false><<<grid, T.threads, T.bytes, s>>>(p);
+  else
+    T.swap ? k_force_staged64<2, 256, true><<<grid, T.threads, T.bytes, s>>>(p)
+           : k_force_staged64<2, 256, false><<<grid, T.threads, T.bytes, s>>>(p);
   VPD_CUDA(cudaGetLastError());
   return VPD_OK;
 }

@@ -28,12 +28,13 @@ constexpr int kGroupBlocks = 256;   // k_integrate blocks reduced together by th
 constexpr int kBondThreads = 256;    // threads per block of the bond kernels
 constexpr int kMaterialThreads = 128;
 constexpr int kMaxStencilWords = 32; // at most 1024 lattice offsets per stencil
-constexpr int kStagedThreads = 128;  // threads per block of the TMA-staged FP64 force kernel
 constexpr size_t kStagedMaxBytes = 110 * 1024;  // its box, so that two blocks fit an SM
 
 // Tiles of the TMA-staged FP64 force kernel (vpd_staged64.cu); bytes == 0: not in use.
 struct StagedTiles {
-  int tz = 0, ty = 0, qy = 0;          // tile extent along z and y; four-point y columns
+  int p = 4;                           // points per thread along y (2 or 4)
+  bool swap = true;                    // record halves read in alternating order
+  int tz = 0, ty = 0, qy = 0;          // tile extent along z and y; p-point y columns
   int ry = 0, rz = 0;                  // the stencil's reach along y and z
   int by = 0, bz = 0;                  // box extent: tile plus reach on both sides
   int tiles_y = 0, tiles_z = 0, threads = 0;
@@ -66,9 +67,9 @@ struct StepParams {
   StencilLayout st;           // lattice-stencil layout; used instead of the ELL when st.nw > 0
   int lat_nx, lat_ny, lat_nz; // the lattice (points in index order (x ny + y) nz + z)
   double lat_h;               // lattice spacing
-  int tiled;                  // bond kernels: 0 per slot; mixed 1 tiled scalar, 4 packed pairs, 2 shared
-                              // windows (packed pairs with damage); FP64 2 tiled with the TMA-staged
-                              // force, 3 tiled with the 2-point force, 5 tiled with the 4-point force
+  int tiled;                  // bond kernels: 0 per slot; mixed 1 tiled scalar, else packed pairs; FP64
+                              // 2 tiled with the TMA-staged force, 3 tiled with the 2-point force,
+                              // else tiled with the 4-point force
   // kinematic state
   double4 *u0, *u1;           // displacement ping-pong: increment s reads u[s & 1]
   double4 *vel, *acc, *force;
@@ -164,10 +165,8 @@ int launch_deformation_mixed(const StepParams &p, cudaStream_t s);
 int launch_force_mixed(const StepParams &p, cudaStream_t s);
 int launch_mixed_setup(const StepParams &p, int ny, int nz, double h, double yoff, double zoff,
                        cudaStream_t s);
-// tiled mixed-precision bond kernels (vpd_tiled.cu; the shared-window deformation kernel in
-// vpd_window.cu)
+// tiled mixed-precision bond kernels (vpd_tiled.cu)
 int launch_deformation_tiled(const StepParams &p, cudaStream_t s);
-int launch_deformation_window(const StepParams &p, cudaStream_t s);
 int launch_force_tiled(const StepParams &p, cudaStream_t s);
 // tiled FP64 bond kernels (vpd_tiled64.cu)
 int launch_deformation_tiled64(const StepParams &p, cudaStream_t s);

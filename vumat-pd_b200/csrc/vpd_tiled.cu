@@ -567,37 +567,7 @@ __device__ __forceinline__ void force_pair_window(const StepParams &p, int cnt, 
   }
 }
 
-// Window position t of a group whose bonds are all present and intact for both points: no bond
-// weights, each row's dot product accumulated straight into the partial sum.
-template <typename I>
-__device__ __forceinline__ void force_pair_element_full(const StepParams &p, int t, I j, float gx, float gz,
-                                                        float by0, float h, const ForcePair &pt, float2 (&part)[3]) {
-  const float4 a = ldgf4(p.fmapf + j), b = ldgf4(p.fmapf + p.n + j), c = ldgf4(p.fmapf + 2 * p.n + j);
-  const float bx = a.w + gx, by = b.w + fmaf((float)t, h, by0), bz = c.w + gz;
-  const float2 e0 = sub2(bcast2(bx), pt.jx), e1 = sub2(bcast2(by), pt.jy), e2 = sub2(bcast2(bz), pt.jz);
-  part[0] = __ffma2_rn(bcast2(a.z), e2, __ffma2_rn(bcast2(a.y), e1, __ffma2_rn(bcast2(a.x), e0, part[0])));
-  part[1] = __ffma2_rn(bcast2(b.z), e2, __ffma2_rn(bcast2(b.y), e1, __ffma2_rn(bcast2(b.x), e0, part[1])));
-  part[2] = __ffma2_rn(bcast2(c.z), e2, __ffma2_rn(bcast2(c.y), e1, __ffma2_rn(bcast2(c.x), e0, part[2])));
-}
-
-template <int CNT, typename I>
-__device__ __forceinline__ void force_full_window(const StepParams &p, int cnt, I jb, I nz, float gx, float gz,
-                                                  float by0, float h, const ForcePair &pt, const uint32_t (&bits)[2],
-                                                  float2 (&part)[3]) {
-  if constexpr (CNT > 0) {
-#pragma unroll
-    for (int t = 1; t < CNT; ++t)
-      force_pair_element_full<I>(p, t, jb + (I)t * nz, gx, gz, by0, h, pt, part);
-    force_pair_ends<CNT, I>(p, jb, jb + (I)CNT * nz, gx, gz, by0, h, pt, bits, part);
-  } else {
-    for (int t = 0; t < cnt + 1; ++t)  // within the zero halo of the neighbour arrays
-      force_pair_element<I>(p, t, jb + (I)t * nz, gx, gz, by0, h, pt, bits, part);
-  }
-}
-
 // f = sum (V_j M_j) xi over intact bonds + M_i s_i with s_i = vxi_i - sum_{broken j} V_j xi.
-// Groups whose bonds are all present and intact for both points of every thread of the warp
-// (p.tiled == 2, the default) skip the bond weights (force_full_window).
 // Three blocks per SM (85 registers, a few bytes of spills): the gathers' latency wants the
 // warps more than the unrolled windows want registers (6 % faster than at two blocks on the
 // 1M-point bar; 8 % with damage).
@@ -662,22 +632,7 @@ __global__ void __launch_bounds__(kBondThreads, 3) k_force_pair(const __grid_con
     const float gx = (float)gr.x * h, gz = (float)gr.y * h, by0 = (float)gr.z * h;
     const int64_t jb = ((int64_t)(x + gr.x) * ny + (yb * 2 + gr.z)) * nz + (z + gr.y);
     float2 part[3] = {make_float2(0.0f, 0.0f), make_float2(0.0f, 0.0f), make_float2(0.0f, 0.0f)};
-    const bool full = (bits[0] == cm || !vp[0]) && (bits[1] == (cm << 1) || !vp[1]);
-    if (UNROLL && p.tiled == 2 && __all_sync(0xffffffffu, full)) {
-      const int jb32 = (int)jb, nz32 = nz;
-#define VPD_FULL_CASE(C)                                                                  \
-  case C:                                                                                 \
-    force_full_window<C, int>(p, cnt, jb32, nz32, gx, gz, by0, h, pt, bits, part);       \
-    break;
-      switch (cnt) {
-        VPD_FULL_CASE(1) VPD_FULL_CASE(2) VPD_FULL_CASE(3) VPD_FULL_CASE(4)
-        VPD_FULL_CASE(5) VPD_FULL_CASE(6) VPD_FULL_CASE(7) VPD_FULL_CASE(8)
-        VPD_FULL_CASE(9) VPD_FULL_CASE(10) VPD_FULL_CASE(11) VPD_FULL_CASE(12)
-      default:
-        force_full_window<0, int>(p, cnt, jb32, nz32, gx, gz, by0, h, pt, bits, part);
-      }
-#undef VPD_FULL_CASE
-    } else if (UNROLL) {
+    if (UNROLL) {
       static_assert(kUnrolledSlots == 12, "the cases below list the unrolled slot counts");
       const int jb32 = (int)jb, nz32 = nz, n32 = (int)n;
 #define VPD_FORCE_CASE(C)                                                                 \
@@ -735,12 +690,9 @@ template <bool UNROLL> static void launch_deformation(const StepParams &p, cudaS
   }
 }
 
-// p.tiled: 1 the scalar two-point kernels, 4 the packed-pair ones, 2 (the default) the
-// shared-window kernel of vpd_window.cu without bond damage and the packed-pair one with it
-// (VPD_BOND_KERNEL, read when the handle is created)
+// p.tiled: 1 the scalar two-point kernels, else the packed-pair ones (VPD_BOND_KERNEL, read
+// when the handle is created)
 int launch_deformation_tiled(const StepParams &p, cudaStream_t s) {
-  if (p.tiled == 2 && !p.damage)
-    return launch_deformation_window(p, s);
   index32(p) ? launch_deformation<true>(p, s) : launch_deformation<false>(p, s);
   VPD_CUDA(cudaGetLastError());
   return VPD_OK;
