@@ -75,6 +75,7 @@ def oracle_lib():
         lib.vo_jitter_value.argtypes = [ctypes.c_uint64, ctypes.c_int64, ctypes.c_int,
                                         ctypes.c_double]
         lib.vo_ramp.argtypes = [ctypes.POINTER(VpdCase), ctypes.c_double, _D]
+        lib.vo_set_perturbation.argtypes = [ctypes.c_int]
         _oracle = lib
     return _oracle
 
@@ -291,6 +292,12 @@ def damage(pos, disp, vol, row_ptr, col, initiation, failure, bond_damage):
                                 row_ptr.ctypes.data_as(_I64), col.ctypes.data_as(_I32),
                                 initiation, failure, _dp(bd), _dp(idx))
     return rc, bd, idx
+
+
+def set_perturbation(every):
+    """Plants a one-ulp change in the deformation sum of every `every`-th point (0: none); for
+    the sensitivity test only."""
+    oracle_lib().vo_set_perturbation(int(every))
 
 
 def jitter_value(seed, p, c, amp):

@@ -215,6 +215,13 @@ int vo_shape_inverse(int64_t n, const double *pos, const double *vol, const int6
   return status;
 }
 
+/* A planted rounding change for the sensitivity test (tests/test_oracle.py): when every > 0,
+   the first component of the deformation sum of each point i with i % every == 3 is moved up
+   by one unit in the last place before F is formed. 0 (the default) leaves the reference's
+   arithmetic untouched. */
+static int g_perturb_every = 0;
+void vo_set_perturbation(int every) { g_perturb_every = every; }
+
 /* computeDeformationGradients, :172-197 */
 int vo_deformation(int64_t n, const double *pos, const double *disp, const double *vol,
                    const int64_t *row_ptr, const int32_t *col, const double *kinv, double *F) {
@@ -234,6 +241,8 @@ int vo_deformation(int64_t n, const double *pos, const double *disp, const doubl
         for (int b = 0; b < 3; ++b)
           num[3 * a + b] += vol[j] * yij[a] * xi[b];
     }
+    if (g_perturb_every > 0 && i % g_perturb_every == 3)
+      num[0] = nextafter(num[0], INFINITY);
     m_mul(num, kinv + 9 * i, F + 9 * i);
   }
   return VPD_OK;

@@ -256,12 +256,13 @@ def test_sliced_ell_layout_matches_stencil_layout(monkeypatch):
 
 
 @pytest.mark.parametrize("dims", [(24, 21, 17), (12, 37, 70)])
-@pytest.mark.parametrize("kind", ["", "tiled4", "tiled2"])
+@pytest.mark.parametrize("kind", ["", "staged", "staged4", "tiled2"])
 @pytest.mark.parametrize("damage", [0, 1])
 def test_tiled_fp64_bond_kernels_match_slot_kernels_bitwise(monkeypatch, damage, kind, dims):
-    """The tiled FP64 bond kernels (two points per thread along y; in the force kernel four,
-    from shared memory filled plane by plane by TMA by default, from L1 with tiled4, two with
-    tiled2) sum every point's bonds in the per-slot kernels' order with the same operations:
+    """The tiled FP64 bond kernels (two points per thread along y; in the force kernel four
+    through L1 by default, two with tiled2, or two or four from a shared-memory box filled plane
+    by plane by TMA with staged) sum every point's bonds in the per-slot kernels' order with
+    the same operations:
     on the jittered horizon-4 bar (y extent 21 and z extent 17, so the last tiles are ragged)
     the increments agree bit for bit, bond breaking included. The second lattice (z extent 70)
     takes three staged tiles along z and three along y, the last of each ragged."""
@@ -273,7 +274,9 @@ def test_tiled_fp64_bond_kernels_match_slot_kernels_bitwise(monkeypatch, damage,
     with vpd.Simulation(case) as a:
         ra = a.step(150)
         fa = {f: a.field(f) for f in fields}
-    monkeypatch.setenv("VPD_BOND_KERNEL", kind)
+    monkeypatch.setenv("VPD_BOND_KERNEL", "staged" if kind.startswith("staged") else kind)
+    if kind == "staged4":
+        monkeypatch.setenv("VPD_STAGED", "4x128")
     with vpd.Simulation(case) as b:
         rb = b.step(150)
         for f in fields:

@@ -441,22 +441,17 @@ int create_impl(vpd_handle *h, const vpd_case *c, const double *positions, const
   p.lat_nx = c->nx, p.lat_ny = c->ny, p.lat_nz = c->nz, p.lat_h = c->spacing;
   {
     // VPD_BOND_KERNEL=slot selects the per-slot bond kernels (both precisions), scalar the
-    // two-point tiled mixed kernels in scalar FP32, tiled2 and tiled4 the two- and four-point
-    // FP64 force kernels reading through L1 (default: tiled; packed pairs when mixed; the
-    // TMA-staged FP64 force kernel)
+    // two-point tiled mixed kernels in scalar FP32, tiled2 the two-point FP64 force kernel,
+    // staged the TMA-staged FP64 force kernel (default: tiled; packed pairs when mixed, four
+    // points per thread reading through L1 in the FP64 force)
     const char *bk = getenv("VPD_BOND_KERNEL");
     const std::string kind = bk ? bk : "";
-    p.tiled = kind == "slot" ? 0
-              : kind == "scalar" ? 1
-              : kind == "tiled2" ? 3
-              : kind == "pair"   ? 4
-              : kind == "tiled4" ? 5
-                                 : 2;
+    p.tiled = kind == "slot" ? 0 : kind == "scalar" ? 1 : kind == "tiled2" ? 3 : kind == "staged" ? 6 : 2;
   }
   if (p.st.nw && ((rc = dalloc(h, &p.vxi, n)) ||
                   (c->precision != VPD_PRECISION_MIXED && (rc = dalloc(h, &p.fmap, 3 * n)))))
     return rc;
-  if (p.st.nw && p.fmap && p.tiled == 2 && (rc = setup_staged_force64(p, p.st.rx, p.st.ry, p.st.rz)))
+  if (p.st.nw && p.fmap && p.tiled == 6 && (rc = setup_staged_force64(p, p.st.rx, p.st.ry, p.st.rz)))
     return rc;
   p.nstatev = c->nstatev;
   p.flags = h->flags, p.obsw = h->obsw;

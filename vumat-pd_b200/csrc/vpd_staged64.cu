@@ -1,9 +1,14 @@
 // TMA-staged FP64 force bond sum of the plain path: k_force_tiled64's arithmetic with the
 // neighbours' force-map records read from shared memory instead of through L1.
 //
-// A block owns a tile of one lattice plane x: Ty x Tz points (y, z), each thread four
-// consecutive y of one z (the tiling of k_force_tiled64<4>, whose window arithmetic and slot
-// order it keeps, so the result is bit-identical to the per-slot kernel k_force_stencil).
+// Selected with VPD_BOND_KERNEL=staged; the default FP64 force kernel is k_force_tiled64<4>,
+// which reads the same records through L1: on the 1M-point bar this kernel takes 0.85 ms per
+// increment against 0.81 ms for the L1 kernel (measured on a B200; the box of 96-byte records
+// with its halo limits the block to two per SM, and the L1 already serves the gathers).
+//
+// A block owns a tile of one lattice plane x: Ty x Tz points (y, z), each thread P consecutive
+// y of one z (the tiling of k_force_tiled64<P>, whose window arithmetic and slot order it
+// keeps, so the result is bit-identical to the per-slot kernel k_force_stencil).
 // The stencil's groups come plane by plane (ascending x offset dx). For each plane x + dx one
 // thread issues a single cp.async.bulk.tensor load of the tile's neighbourhood of that plane:
 // a box of (Ty + 2 ry) x (Tz + 2 rz) points of all three force-map rows (a 5-D tensor map over
@@ -11,6 +16,8 @@
 // lattice, completing on an mbarrier. The block then sums every group of that plane from the
 // box and, after a barrier, the next plane's load overwrites it. Planes past either end of
 // the bar are skipped. Two blocks per SM keep one block's load in flight while the other sums.
+// Planes are loaded in x-offset order (dx ascending) because the groups, and so the slot order
+// the sums keep, come that way.
 //
 // Every wait is bounded: a timed-out wait sets STATUS_STAGED_WAIT, waits once more (bounded)
 // for the copy in flight and the block returns; the host reports VPD_ERR_CUDA. A box base that
@@ -230,23 +237,18 @@ __global__ void __launch_bounds__(THREADS, 2) k_force_staged64(const __grid_cons
 
 }  // namespace
 
-// The kernel's variants: points per thread along y, threads per block, halves read in
-// alternating order (VPD_STAGED: "4x128s" the default, "4x128", "2x256s", "2x256").
+// The kernel's variants: two points per thread along y and 256 threads (the default), or four
+// and 128 (VPD_STAGED=4x128); the record halves are read in alternating order in both (without
+// it the 1M-point bar's force pass took 1.19 against 0.85 ms with two points per thread).
 struct StagedVariant {
   int p, threads;
-  bool swap;
 };
 
 static StagedVariant staged_variant() {
   const char *v = getenv("VPD_STAGED");
-  const std::string s = v ? v : "";
-  if (s == "4x128")
-    return {4, 128, false};
-  if (s == "2x256s")
-    return {2, 256, true};
-  if (s == "2x256")
-    return {2, 256, false};
-  return {4, 128, true};
+  if (v && std::string(v) == "4x128")
+    return {4, 128};
+  return {2, 256};
 }
 
 template <int P, int THREADS, bool SWAP> static int set_smem(size_t bytes) {
@@ -266,7 +268,7 @@ int setup_staged_force64(StepParams &p, int rx, int ry, int rz) {
     return VPD_OK;
   const StagedVariant V = staged_variant();
   StagedTiles T{};
-  T.p = V.p, T.swap = V.swap;
+  T.p = V.p;
   T.tz = p.lat_nz <= 64 ? p.lat_nz : 32;
   const int cols_y = (p.lat_ny + V.p - 1) / V.p;
   T.qy = std::max(1, std::min(V.threads / T.tz, cols_y));
@@ -300,8 +302,7 @@ int setup_staged_force64(StepParams &p, int rx, int ry, int rz) {
       CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS)
     return set_error(VPD_ERR_CUDA, "cuTensorMapEncodeTiled failed for the force map");
-  int rc = V.p == 4 ? (V.swap ? set_smem<4, 128, true>(bytes) : set_smem<4, 128, false>(bytes))
-                    : (V.swap ? set_smem<2, 256, true>(bytes) : set_smem<2, 256, false>(bytes));
+  int rc = V.p == 4 ? set_smem<4, 128, true>(bytes) : set_smem<2, 256, true>(bytes);
   if (rc)
     return rc;
   p.staged = T;
@@ -312,11 +313,9 @@ int launch_force_staged64(const StepParams &p, cudaStream_t s) {
   const StagedTiles &T = p.staged;
   const unsigned grid = (unsigned)((int64_t)p.lat_nx * T.tiles_y * T.tiles_z);
   if (T.p == 4)
-    T.swap ? k_force_staged64<4, 128, true><<<grid, T.threads, T.bytes, s>>>(p)
-           : k_force_staged64<4, 128, false><<<grid, T.threads, T.bytes, s>>>(p);
+    k_force_staged64<4, 128, true><<<grid, T.threads, T.bytes, s>>>(p);
   else
-    T.swap ? k_force_staged64<2, 256, true><<<grid, T.threads, T.bytes, s>>>(p)
-           : k_force_staged64<2, 256, false><<<grid, T.threads, T.bytes, s>>>(p);
+    k_force_staged64<2, 256, true><<<grid, T.threads, T.bytes, s>>>(p);
   VPD_CUDA(cudaGetLastError());
   return VPD_OK;
 }

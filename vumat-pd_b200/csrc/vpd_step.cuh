@@ -32,8 +32,7 @@ constexpr size_t kStagedMaxBytes = 110 * 1024;  // its box, so that two blocks f
 
 // Tiles of the TMA-staged FP64 force kernel (vpd_staged64.cu); bytes == 0: not in use.
 struct StagedTiles {
-  int p = 4;                           // points per thread along y (2 or 4)
-  bool swap = true;                    // record halves read in alternating order
+  int p = 2;                           // points per thread along y (2 or 4)
   int tz = 0, ty = 0, qy = 0;          // tile extent along z and y; p-point y columns
   int ry = 0, rz = 0;                  // the stencil's reach along y and z
   int by = 0, bz = 0;                  // box extent: tile plus reach on both sides
@@ -68,8 +67,8 @@ struct StepParams {
   int lat_nx, lat_ny, lat_nz; // the lattice (points in index order (x ny + y) nz + z)
   double lat_h;               // lattice spacing
   int tiled;                  // bond kernels: 0 per slot; mixed 1 tiled scalar, else packed pairs; FP64
-                              // 2 tiled with the TMA-staged force, 3 tiled with the 2-point force,
-                              // else tiled with the 4-point force
+                              // tiled with the 4-point force, 3 with the 2-point force, 6 with the
+                              // TMA-staged force
   // kinematic state
   double4 *u0, *u1;           // displacement ping-pong: increment s reads u[s & 1]
   double4 *vel, *acc, *force;

@@ -293,10 +293,10 @@ int launch_deformation_tiled64(const StepParams &p, cudaStream_t s) {
   return VPD_OK;
 }
 
-// the TMA-staged kernel (vpd_staged64.cu) where its box fits, else four points per thread
-// (two with VPD_BOND_KERNEL=tiled2)
+// four points per thread (two with VPD_BOND_KERNEL=tiled2; the TMA-staged kernel of
+// vpd_staged64.cu with VPD_BOND_KERNEL=staged where its box fits)
 int launch_force_tiled64(const StepParams &p, cudaStream_t s) {
-  if (p.tiled == 2 && p.staged.bytes)
+  if (p.tiled == 6 && p.staged.bytes)
     return launch_force_staged64(p, s);
   if (p.tiled == 3) {
     const unsigned grid = tiled_grid<2>(p);
