@@ -16,7 +16,8 @@ deformation sum of every seventh point moved by one unit in the last place drift
 archive by several 1e-6 (tests/test_oracle.py::test_archived_shared_case_is_sensitive_to_one_ulp),
 and the device sums the same bonds with other roundings (FMA, the stencil's slot order), so for
 them the bar is the one such a rounding change meets: stress NRMSE below 3e-5, the other
-quantities within 1e-4 (measured 4e-6 to 1.1e-5 for the stress history).
+quantities within 1e-4 (measured 4e-6 to 1.1e-5 for the stress history), and the analysis
+metrics at verify_metrics.py's 0.5 % except final_stress_pct (see the test).
 """
 import json
 import math
@@ -80,6 +81,15 @@ def test_archived_case_runs_on_the_gpu(archive, name, tmp_path):
     assert m["earlyElasticSlope_MPa"] == pytest.approx(slope, rel=tol_sum)
 
     got = VM.run_metrics(str(tmp_path), ref)
-    assert VM.mismatches(expected[name], got) == [], (got, expected[name])
-    for k in ("stress_history_pct", "displacement_pct", "max_eqps_pct", "final_stress_pct"):
+    if not chaotic:
+        assert VM.mismatches(expected[name], got) == [], (got, expected[name])
+    else:
+        # final_stress_pct is the difference of two nearly equal final stresses (0.06-0.2 %), so
+        # a 1e-5 change of the final stress moves it by 1-2 %: the reference's own run with the
+        # one-ulp change of the sensitivity test moves it by 1.4 % (pd_shared) and 1.9 %
+        # (pd_delta2). It is checked through the final stress itself and in percentage points.
+        assert VM.mismatches({k: v for k, v in expected[name].items() if k != "final_stress_pct"}, got) == []
+        assert abs(got["final_stress_pct"] - expected[name]["final_stress_pct"]) < 0.01
+        assert math.isclose(got["stress_MPa"], expected[name]["stress_MPa"], rel_tol=1e-4)
+    for k in ("stress_history_pct", "displacement_pct", "max_eqps_pct"):
         assert math.isclose(got[k], expected[name][k], rel_tol=1e-2 if chaotic else 1e-5, abs_tol=1e-6), k

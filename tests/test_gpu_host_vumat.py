@@ -48,10 +48,12 @@ def test_host_jc_plugin_matches_device_update(precision):
         temperature = b.field("temperature")
     if precision == "fp64":
         assert ra[-1, vpd.DIAG["max_eqps"]] > 1e-3
+    # mixed: FP32 bond sums carry the plugin's last-bit differences a little further
+    tol = 1e-8 if precision == "fp64" else 1e-7
     assert nrmse(rb[:, STRESS], ra[:, STRESS]) < 1e-9
     for f in ("displacement", "velocity", "stress_corotational"):
-        assert nrmse(fb[f], fa[f]) < 1e-8, f
-    assert nrmse(fb["state"][:, 1], fa["state"][:, 1]) < 1e-8
+        assert nrmse(fb[f], fa[f]) < tol, f
+    assert nrmse(fb["state"][:, 1], fa["state"][:, 1]) < tol
     assert np.isfinite(temperature).all() and temperature.min() >= case.reference_temperature
 
 

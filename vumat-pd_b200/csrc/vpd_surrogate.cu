@@ -18,6 +18,8 @@
 #include "vpd_mlp_tile.cuh"
 #include "vpd_surrogate.cuh"
 
+#include <cstdlib>
+
 #include <algorithm>
 #include <cmath>
 #include <numeric>
@@ -507,8 +509,8 @@ __device__ __noinline__ float sparse_network_guesses(const uint16_t *sw, const f
 // with a yielding point; persistent blocks with the weights staged once).
 enum SurrogateMode { SURR_WARM = 0, SURR_SPARSE = 1, SURR_TENSOR = 2 };
 
-template <int MODE>
-__global__ void __launch_bounds__(kMaterialThreads, MODE == SURR_TENSOR ? 2 : 4)
+template <int MODE, int MINB = (MODE == SURR_TENSOR ? 2 : 4)>
+__global__ void __launch_bounds__(kMaterialThreads, MINB)
     k_material_surrogate(const __grid_constant__ StepParams p) {
   constexpr bool NET = MODE == SURR_TENSOR;
   extern __shared__ __align__(1024) unsigned char smem[];
@@ -621,8 +623,11 @@ __global__ void __launch_bounds__(kMaterialThreads, MODE == SURR_TENSOR ? 2 : 4)
 }
 
 static int g_surrogate_sms = 0;
+static int g_surrogate_minb = 4;
 
 int prepare_material_surrogate() {
+  const char *mb = getenv("VPD_SURR_MINB");
+  g_surrogate_minb = mb && mb[0] == '3' ? 3 : 4;
   int dev = 0;
   VPD_CUDA(cudaGetDevice(&dev));
   VPD_CUDA(cudaDeviceGetAttribute(&g_surrogate_sms, cudaDevAttrMultiProcessorCount, dev));
@@ -640,7 +645,10 @@ int launch_material_surrogate(const StepParams &p, cudaStream_t s) {
     const int64_t grid = std::min<int64_t>(tiles, 2 * (int64_t)g_surrogate_sms);
     k_material_surrogate<SURR_TENSOR><<<(unsigned)grid, kMaterialThreads, kSurrSmem, s>>>(p);
   } else if (p.surr_guess == VPD_GUESS_HYBRID) {
-    k_material_surrogate<SURR_SPARSE><<<(unsigned)tiles, kMaterialThreads, 0, s>>>(p);
+    if (g_surrogate_minb == 3)
+      k_material_surrogate<SURR_SPARSE, 3><<<(unsigned)tiles, kMaterialThreads, 0, s>>>(p);
+    else
+      k_material_surrogate<SURR_SPARSE><<<(unsigned)tiles, kMaterialThreads, 0, s>>>(p);
   } else {
     k_material_surrogate<SURR_WARM><<<(unsigned)tiles, kMaterialThreads, 0, s>>>(p);
   }
