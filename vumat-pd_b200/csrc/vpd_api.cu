@@ -491,10 +491,6 @@ int create_impl(vpd_handle *h, const vpd_case *c, const double *positions, const
   p.part_group = h->part_group, p.group_counter = h->group_counter;
   p.counter = h->counter;
   p.mat_blocks = mat_blocks;
-  {
-    const char *mb = getenv("VPD_MAT_MINB");
-    p.mat_minb = mb && mb[0] == '3' ? 3 : 4;
-  }
   p.interior = sets.interior, p.gauge = sets.gauge, p.lat_gauge = sets.lat_gauge;
   p.area = sets.area, p.n_lat_pos = sets.n_lat_pos, p.n_lat_neg = sets.n_lat_neg;
   p.sign = (c->bc_mode == VPD_BC_SMOOTH_DISPLACEMENT ? c->amplitude : c->grip_velocity) > 0.0 ? 1.0 : -1.0;

@@ -179,10 +179,11 @@ __global__ void __launch_bounds__(kBondThreads) k_deformation(StepParams p) {
 // ------------------------------------------------------------------ k_material
 // Four blocks per SM (128 registers, a few hundred bytes of spills to L1): the FP64 kinematics
 // and return map are latency-bound, and the extra warps outweigh the spills (26 % faster on
-// the 250k-point bar in plastic flow than at the unconstrained 196 registers).
+// the 250k-point bar in plastic flow than at the unconstrained 196 registers; on the 1M-point
+// bar in plastic flow 0.70 ms against 0.76 ms at three blocks per SM).
 // POINT_DAMAGE: the point damage modes (a separate instance, so the plain one keeps its registers).
-template <bool POINT_DAMAGE, int MINB = 4>
-__global__ void __launch_bounds__(kMaterialThreads, MINB) k_material(const __grid_constant__ StepParams p) {
+template <bool POINT_DAMAGE>
+__global__ void __launch_bounds__(kMaterialThreads, 4) k_material(const __grid_constant__ StepParams p) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   double part[PM_COUNT] = {};
   double maxEqps = 0.0;
@@ -574,8 +575,7 @@ int launch_stage(int stage, const StepParams &p, cudaStream_t s) {
     if (p.point_damage)
       k_material<true><<<(unsigned)material_grid(p.n), kMaterialThreads, 0, s>>>(p);
     else
-      p.mat_minb == 3 ? k_material<false, 3><<<(unsigned)material_grid(p.n), kMaterialThreads, 0, s>>>(p)
-                      : k_material<false><<<(unsigned)material_grid(p.n), kMaterialThreads, 0, s>>>(p);
+      k_material<false><<<(unsigned)material_grid(p.n), kMaterialThreads, 0, s>>>(p);
   } else if (stage == 2) {
     if (p.mixed)
       return p.tiled ? launch_force_tiled(p, s) : launch_force_mixed(p, s);

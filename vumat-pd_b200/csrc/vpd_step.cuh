@@ -126,7 +126,6 @@ struct StepParams {
   unsigned int *counter;       // groups done (k_integrate)
   unsigned int *group_counter; // blocks done, per group
   int mat_blocks;
-  int mat_minb;                // blocks per SM the FP64 material kernel is built for (3 or 4)
   // diagnostic constants
   double interior, gauge, lat_gauge, area, sign, n_lat_pos, n_lat_neg;
 };

@@ -18,8 +18,6 @@
 #include "vpd_mlp_tile.cuh"
 #include "vpd_surrogate.cuh"
 
-#include <cstdlib>
-
 #include <algorithm>
 #include <cmath>
 #include <numeric>
@@ -509,6 +507,9 @@ __device__ __noinline__ float sparse_network_guesses(const uint16_t *sw, const f
 // with a yielding point; persistent blocks with the weights staged once).
 enum SurrogateMode { SURR_WARM = 0, SURR_SPARSE = 1, SURR_TENSOR = 2 };
 
+// Blocks per SM: two for the tensor-core variant (its shared-memory weights), three for the
+// hybrid guess (fewer spills of its larger body: 0.399 against 0.423 ms at four blocks on the
+// 1M-point bar in plastic flow), four for the warm start.
 template <int MODE, int MINB = (MODE == SURR_TENSOR ? 2 : 4)>
 __global__ void __launch_bounds__(kMaterialThreads, MINB)
     k_material_surrogate(const __grid_constant__ StepParams p) {
@@ -623,11 +624,8 @@ __global__ void __launch_bounds__(kMaterialThreads, MINB)
 }
 
 static int g_surrogate_sms = 0;
-static int g_surrogate_minb = 4;
 
 int prepare_material_surrogate() {
-  const char *mb = getenv("VPD_SURR_MINB");
-  g_surrogate_minb = mb && mb[0] == '3' ? 3 : 4;
   int dev = 0;
   VPD_CUDA(cudaGetDevice(&dev));
   VPD_CUDA(cudaDeviceGetAttribute(&g_surrogate_sms, cudaDevAttrMultiProcessorCount, dev));
@@ -645,10 +643,7 @@ int launch_material_surrogate(const StepParams &p, cudaStream_t s) {
     const int64_t grid = std::min<int64_t>(tiles, 2 * (int64_t)g_surrogate_sms);
     k_material_surrogate<SURR_TENSOR><<<(unsigned)grid, kMaterialThreads, kSurrSmem, s>>>(p);
   } else if (p.surr_guess == VPD_GUESS_HYBRID) {
-    if (g_surrogate_minb == 3)
-      k_material_surrogate<SURR_SPARSE, 3><<<(unsigned)tiles, kMaterialThreads, 0, s>>>(p);
-    else
-      k_material_surrogate<SURR_SPARSE><<<(unsigned)tiles, kMaterialThreads, 0, s>>>(p);
+    k_material_surrogate<SURR_SPARSE, 3><<<(unsigned)tiles, kMaterialThreads, 0, s>>>(p);
   } else {
     k_material_surrogate<SURR_WARM><<<(unsigned)tiles, kMaterialThreads, 0, s>>>(p);
   }
