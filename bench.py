@@ -7,8 +7,9 @@ surrogate + mixed-precision PD against plain FP64 PD.
 Workload: the 400x50x50 jittered Johnson-Cook tensile bar (1,000,000 points, horizon 4.015 h,
 about 238 bonds per point, grips pulled at 5 m/s) in plastic flow: each mode runs the bar from
 rest for --preload increments (untimed), W warm-up increments, then K timed increments. The
-bar runs without bond damage: with critical-stretch damage the bar fails near increment 450,
-before it yields, so the damaged bar is timed separately from rest (from_rest_with_damage). A
+bar runs without bond damage: with critical-stretch damage its first bonds break near increment
+175, before it yields, and it comes apart by increment ~800, so the damaged bar is timed
+separately from rest (from_rest_with_damage). A
 step is one explicit increment of the whole bar. One process per GPU (torchrun); the path
 does not shard across GPUs, so N GPUs run N independent replicas ("replicas only") and the
 value is the sum of their particle-steps/s, timed as the max over ranks.
@@ -27,6 +28,8 @@ Printed JSON line (rank 0):
                final snapshot fields copied back; host wall clock over all increments
   roofline     the headline mode's dominant kernel: algorithmic bytes / its CUDA-event time
                vs the measured HBM copy bandwidth; traffic from the ncu summary in profiles/
+               (the bond kernels are bound by FP32 issue, not HBM: their FP32 rate rides along)
+  kernels      the same for each of the increment's four kernels
   cpu_baseline the reference library (compiled from its sources into oracle/_ref), all host
                threads, on the same workload: a 40-plane slab of the bar (40x50x50, 100k
                points; same horizon, jitter, heating and grips; no bond damage), run from rest
@@ -148,9 +151,12 @@ class ClockSampler:
 FP32_FLOP_PER_BOND = {"deformation": 27, "force": 24}
 FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # 148 SMs x 128 FP32 lanes x FMA at 1965 MHz
 LIMITER = {
-    "deformation": "FP32 issue: FMA pipe 52 % and throttling, issue 51 % active, 76 B/pt DRAM (ncu)",
-    "force": "FP32 issue and L1 gathers: issue 57 % active, FMA pipe 42 %, L1 71 %, 140 B/pt DRAM (ncu)",
-    "material": "FP64 latency at low occupancy (ncu)",
+    "deformation": "FP32 issue: issue 52 % active, math-pipe throttle, 54 instructions per bond pair, "
+                   "76 B/pt DRAM (ncu)",
+    "force": "FP32 issue and L1 gathers: issue 59 % active, long-scoreboard stalls, L1 hit 87 %, "
+             "140 B/pt DRAM (ncu)",
+    "material": "FP64 and memory latency at 12 warps per SM; DRAM traffic equals its algorithmic bytes (ncu)",
+    "integrate": "memory latency and the two-level diagnostics reduction (ncu)",
 }
 
 
@@ -494,6 +500,12 @@ def run_gpu(args, world, rank, local):
                      "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
                      "traffic": tr, "algorithmic_bytes": alg[dominant] * n,
                      **fp32_roofline(dominant, nb * n, stages[dominant])},
+        "kernels": {k: {"ms": stages[k], "algorithmic_bytes": alg[k] * n,
+                        "achieved_gbs": alg[k] * n / (stages[k] * 1e-3) / 1e9,
+                        "hbm_frac": alg[k] * n / (stages[k] * 1e-3) / 1e9 / peak,
+                        "traffic": (traffic["bytes_per_point"][f"mixed:{k}"] * n
+                                    if traffic and f"mixed:{k}" in traffic.get("bytes_per_point", {}) else None),
+                        **fp32_roofline(k, nb * n, stages[k])} for k in stages},
         "step_roofline": {"algorithmic_bytes": step_alg,
                           "achieved_gbs": step_alg / (ms_step * 1e-3) / 1e9,
                           "frac": step_alg / (ms_step * 1e-3) / 1e9 / peak,

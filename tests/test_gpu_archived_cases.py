@@ -81,7 +81,7 @@ def test_archived_case_runs_on_the_gpu(archive, name, tmp_path):
     max_eqps, reaction, energy_error, slope = data[f"{name}_summary"]
     assert meta["status"] == "pass" and m["status"] == "pass"
     assert m["maxEqps"] == pytest.approx(max_eqps, rel=tol_sum)
-    assert m["finalReaction_N"] == pytest.approx(reaction, rel=tol_sum)
+    assert m["finalReaction_N"] == pytest.approx(reaction, rel=10 * tol_sum if chaotic else tol_sum)
     assert m["finalEnergyError"] == pytest.approx(energy_error, rel=10 * tol_sum)
     assert m["earlyElasticSlope_MPa"] == pytest.approx(slope, rel=tol_sum)
 

@@ -16,8 +16,9 @@
 // neighbour index is 32-bit. Larger groups, and lattices of 2^30 points or more, take the same
 // body in a runtime loop with 64-bit indices.
 //
-// Arithmetic is that of vpd_mixed.cu: FP32 bond terms, per-group partial sums (folded with
-// Kahan compensation into the force, and in the packed-pair kernels into the deformation sum),
+// Arithmetic is that of vpd_mixed.cu: FP32 bond terms, partial sums per group (per stencil
+// plane in the packed-pair kernels) folded with Kahan compensation into the force (and in the
+// packed-pair kernels into the deformation sum),
 // the FP32 stretch test with a 1e-5 margin and the exact FP64 test inside it, pairs broken once
 // by the lower-index point.
 #include "vpd_bond.cuh"
@@ -433,16 +434,26 @@ __global__ void __launch_bounds__(kBondThreads, 2) k_deformation_pair(const __gr
   pt.jz = make_float2(pa[0].z, pa[1].z);
   pt.ux = make_float2(pb[0].x, pb[1].x), pt.uy = make_float2(pb[0].y, pb[1].y);
   pt.uz = make_float2(pb[0].z, pb[1].z);
-  float2 G[9], Gc[9];  // the sum of the group partials, with Kahan compensation
+  // The windows of one stencil plane (the groups with the same x offset, which come in order)
+  // sum into the plane partial `part`; each plane's partial is folded into G with Kahan
+  // compensation (Gc).
+  float2 G[9], Gc[9], part[9];
 #pragma unroll
   for (int c = 0; c < 9; ++c)
-    G[c] = Gc[c] = make_float2(0.0f, 0.0f);
+    G[c] = Gc[c] = part[c] = make_float2(0.0f, 0.0f);
   int word = -1;  // the mask word held in mw (groups come in slot order: several per word)
+  int plane = INT_MIN;
   uint32_t mw[2] = {0u, 0u};
   for (int g = 0; g < p.st.ngroups; ++g) {
     const int4 gr = __ldg(p.st.groups + g);  // dx, dz, lowest dy, (slots << 16) | first slot
     const int cnt = gr.w >> 16, pos = gr.w & 0xffff, wd = pos >> 5, sh = pos & 31;
     const uint32_t cm = cnt >= 32 ? ~0u : ((1u << cnt) - 1u);
+    if (gr.x != plane) {  // uniform: a new plane; fold the last one's partial
+      plane = gr.x;
+#pragma unroll
+      for (int c = 0; c < 9; ++c)
+        kahan_add2(G[c], Gc[c], part[c]), part[c] = make_float2(0.0f, 0.0f);
+    }
     if (wd != word) {  // uniform: the group table is the same for every thread
       word = wd;
 #pragma unroll
@@ -465,10 +476,6 @@ __global__ void __launch_bounds__(kBondThreads, 2) k_deformation_pair(const __gr
       continue;
     const float gx = (float)gr.x * h, gz = (float)gr.y * h, by0 = (float)gr.z * h;
     const int64_t jb = ((int64_t)(x + gr.x) * ny + (yb * 2 + gr.z)) * nz + (z + gr.y);
-    float2 part[9];
-#pragma unroll
-    for (int c = 0; c < 9; ++c)
-      part[c] = make_float2(0.0f, 0.0f);
     uint32_t fresh[2] = {0u, 0u}, near[2] = {0u, 0u};
     if (UNROLL) {
       static_assert(kUnrolledSlots == 12, "the cases below list the unrolled slot counts");
@@ -491,9 +498,6 @@ __global__ void __launch_bounds__(kBondThreads, 2) k_deformation_pair(const __gr
       deform_pair_window<0, DAMAGE, int64_t>(p, cnt, jb, (int64_t)nz, n, gx, gz, by0, h, pt, bits, live, part,
                                              fresh, near);
     }
-#pragma unroll
-    for (int c = 0; c < 9; ++c)
-      kahan_add2(G[c], Gc[c], part[c]);
     if (DAMAGE)
 #pragma unroll
       for (int q = 0; q < 2; ++q)
@@ -501,6 +505,7 @@ __global__ void __launch_bounds__(kBondThreads, 2) k_deformation_pair(const __gr
   }
 #pragma unroll
   for (int c = 0; c < 9; ++c) {
+    kahan_add2(G[c], Gc[c], part[c]);
     const float2 g = sub2(G[c], Gc[c]);
     if (vp[0])
       p.Gf[c * n + ip[0]] = g.x;
@@ -598,11 +603,20 @@ __global__ void __launch_bounds__(kBondThreads, 3) k_force_pair(const __grid_con
   for (int c = 0; c < 3; ++c)
     fs[c] = fc[c] = make_float2(0.0f, 0.0f), corr[0][c] = corr[1][c] = 0.0;
   int word = -1;  // the mask word held in mw (groups come in slot order: several per word)
+  int plane = INT_MIN;
   uint32_t mw[2] = {0u, 0u};
+  // the windows of one stencil plane sum into `part`, folded into fs with Kahan compensation
+  float2 part[3] = {make_float2(0.0f, 0.0f), make_float2(0.0f, 0.0f), make_float2(0.0f, 0.0f)};
   for (int g = 0; g < p.st.ngroups; ++g) {
     const int4 gr = __ldg(p.st.groups + g);
     const int cnt = gr.w >> 16, pos = gr.w & 0xffff, wd = pos >> 5, sh = pos & 31;
     const uint32_t cm = cnt >= 32 ? ~0u : ((1u << cnt) - 1u);
+    if (gr.x != plane) {  // uniform: a new plane
+      plane = gr.x;
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+        kahan_add2(fs[c], fc[c], part[c]), part[c] = make_float2(0.0f, 0.0f);
+    }
     if (wd != word) {  // uniform: the group table is the same for every thread
       word = wd;
 #pragma unroll
@@ -631,7 +645,6 @@ __global__ void __launch_bounds__(kBondThreads, 3) k_force_pair(const __grid_con
       continue;
     const float gx = (float)gr.x * h, gz = (float)gr.y * h, by0 = (float)gr.z * h;
     const int64_t jb = ((int64_t)(x + gr.x) * ny + (yb * 2 + gr.z)) * nz + (z + gr.y);
-    float2 part[3] = {make_float2(0.0f, 0.0f), make_float2(0.0f, 0.0f), make_float2(0.0f, 0.0f)};
     if (UNROLL) {
       static_assert(kUnrolledSlots == 12, "the cases below list the unrolled slot counts");
       const int jb32 = (int)jb, nz32 = nz, n32 = (int)n;
@@ -650,10 +663,10 @@ __global__ void __launch_bounds__(kBondThreads, 3) k_force_pair(const __grid_con
     } else {
       force_pair_window<0, int64_t>(p, cnt, jb, (int64_t)nz, n, gx, gz, by0, h, pt, bits, part);
     }
-#pragma unroll
-    for (int c = 0; c < 3; ++c)
-      kahan_add2(fs[c], fc[c], part[c]);
   }
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+    kahan_add2(fs[c], fc[c], part[c]);
 #pragma unroll
   for (int q = 0; q < 2; ++q) {
     if (!vp[q])
