@@ -61,6 +61,9 @@ SAMPLE_NX = 40  # CPU sample: 40x50x50 slab of the bar
 # in each increment from here on (the 1M-point bar of the headline: about 70 % from increment
 # 2000 on).
 SAMPLE_PRELOAD = 240
+# The workload both arms name in config.workload (the reference arm times a sample of it).
+WORKLOAD = ("tensile_bar_3 in plastic flow: 400x50x50 jittered (+-0.05 h) steel Johnson-Cook bar, "
+            "horizon 4.015 h, grips 5 m/s, no bond damage")
 
 
 def parse_args():
@@ -289,8 +292,7 @@ def run_reference(args, world, rank):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": base["ms_per_step"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "tensile_bar_3 in plastic flow (400x50x50 jittered steel JC bar, no bond "
-                               "damage), CPU sample",
+        "config": {"workload": WORKLOAD,
                    "sample": base["sample"], "plastic_fraction": base["plastic_fraction"],
                    "ms_per_step": "per increment of the sample"},
         "cpu_baseline": {k: base[k] for k in ("value", "unit", "cores", "kind", "sample", "stage_seconds",
@@ -477,8 +479,7 @@ def run_gpu(args, world, rank, local):
         "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 bonds / f64 state, bf16 network", "data": "synthetic",
-        "config": {"workload": "tensile_bar_3 in plastic flow: 400x50x50 jittered (+-0.05 h) steel "
-                               "Johnson-Cook bar, horizon 4.015 h, grips 5 m/s, no bond damage",
+        "config": {"workload": WORKLOAD,
                    "points": n, "bonds_per_point": round(nb, 2), "mode": "surrogate_mixed",
                    "material": "learned return map (hybrid guess, 2 Newton steps, VUMAT fallback)",
                    "bond_layout_words": nw, "increments": f"{P + W + 1}-{P + W + K} from rest",

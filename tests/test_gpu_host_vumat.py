@@ -48,9 +48,10 @@ def test_host_jc_plugin_matches_device_update(precision):
         temperature = b.field("temperature")
     if precision == "fp64":
         assert ra[-1, vpd.DIAG["max_eqps"]] > 1e-3
-    # mixed: FP32 bond sums carry the plugin's last-bit differences further (velocities ~1e-6)
+    # mixed: FP32 bond sums carry the plugin's last-bit differences further (stress ~2e-9,
+    # velocities ~1e-6)
     tol = 1e-8 if precision == "fp64" else 1e-5
-    assert nrmse(rb[:, STRESS], ra[:, STRESS]) < 1e-9
+    assert nrmse(rb[:, STRESS], ra[:, STRESS]) < (1e-9 if precision == "fp64" else 1e-7)
     for f in ("displacement", "velocity", "stress_corotational"):
         assert nrmse(fb[f], fa[f]) < tol, f
     assert nrmse(fb["state"][:, 1], fa["state"][:, 1]) < tol
