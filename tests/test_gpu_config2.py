@@ -2,7 +2,7 @@
 3.015 h, grips at 1 m/s, critical stretch 0.02) over its full 5000 increments, mixed precision
 (FP32 bond sums, Kahan-compensated) against the plain FP64 path as the GPU oracle.
 
-The bar yields from about increment 2500; its first bonds break near increment 4450 and the
+The bar yields from about increment 2500; its first bonds break near increment 4300 and the
 failure then runs through the whole bar: by increment 5000 practically every bond is broken in
 both runs, and the stresses of the broken-up bar are meaningless. So the stress history is
 compared up to the onset of failure (tolerance 0.5 %, measured ~3e-8), the onset is compared
