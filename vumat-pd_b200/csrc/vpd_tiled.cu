@@ -341,14 +341,26 @@ struct DeformPair {
   float2 jx, jy, jz, ux, uy, uz;  // lane q: point q (jy includes q h)
 };
 
+// The group's offsets of a neighbour from the thread's points: lane q of cx is gx - x_q (the
+// group's x offset times h less point q's jitter), cy the same along y at window position 0
+// (lowest dy times h less y_q, which includes q h), cz along z; window position t adds t h to
+// cy. A bond's reference vector is then the neighbour's jitter plus these, one paired add per
+// component. (The force kernel keeps its per-position adds: at its 85-register budget the three
+// pairs spilled and cost it 11 %, 0.457 against 0.411 ms at 1M points; the deformation kernel
+// gained 2.5 %.)
+struct GroupOffsets {
+  float2 cx, cy, cz;
+};
+
 template <bool DAMAGE, typename I>
-__device__ __forceinline__ void deform_pair_element(const StepParams &p, int t, I j, float gx, float gz, float by0,
+__device__ __forceinline__ void deform_pair_element(const StepParams &p, int t, I j, const GroupOffsets &o,
                                                     float h, const DeformPair &pt, const uint32_t (&bits)[2],
                                                     const uint32_t (&live)[2], float2 (&part)[9],
                                                     uint32_t (&fresh)[2], uint32_t (&near)[2]) {
   const float4 a = ldgf4(p.jit + j), b = ldgf4(p.uf + j);
-  const float bx = a.x + gx, by = a.y + fmaf((float)t, h, by0), bz = a.z + gz;
-  const float2 e0 = sub2(bcast2(bx), pt.jx), e1 = sub2(bcast2(by), pt.jy), e2 = sub2(bcast2(bz), pt.jz);
+  const float2 e0 = __fadd2_rn(bcast2(a.x), o.cx);
+  const float2 e1 = __fadd2_rn(bcast2(a.y), __ffma2_rn(bcast2((float)t), bcast2(h), o.cy));
+  const float2 e2 = __fadd2_rn(bcast2(a.z), o.cz);
   const float2 d0 = sub2(bcast2(b.x), pt.ux), d1 = sub2(bcast2(b.y), pt.uy), d2 = sub2(bcast2(b.z), pt.uz);
   // bit t of bits[q]: window position t is a bond of point q (clear where it holds no slot of q)
   const float2 v = make_float2(((bits[0] >> t) & 1u) ? a.w : 0.0f, ((bits[1] >> t) & 1u) ? a.w : 0.0f);
@@ -370,14 +382,14 @@ __device__ __forceinline__ void deform_pair_element(const StepParams &p, int t, 
 // slot), lane 1 position CNT (point 1's last slot), each with the operations of
 // deform_pair_element, so a window costs CNT pair elements instead of CNT + 1.
 template <int CNT, bool DAMAGE, typename I>
-__device__ __forceinline__ void deform_pair_ends(const StepParams &p, I j0, I j1, float gx, float gz, float by0,
-                                                 float h, const DeformPair &pt, const uint32_t (&bits)[2],
+__device__ __forceinline__ void deform_pair_ends(const StepParams &p, I j0, I j1, const GroupOffsets &o, float h,
+                                                 const DeformPair &pt, const uint32_t (&bits)[2],
                                                  const uint32_t (&live)[2], float2 (&part)[9], uint32_t (&fresh)[2],
                                                  uint32_t (&near)[2]) {
   const float4 a0 = ldgf4(p.jit + j0), b0 = ldgf4(p.uf + j0), a1 = ldgf4(p.jit + j1), b1 = ldgf4(p.uf + j1);
-  const float2 e0 = make_float2((a0.x + gx) - pt.jx.x, (a1.x + gx) - pt.jx.y);
-  const float2 e1 = make_float2((a0.y + fmaf(0.0f, h, by0)) - pt.jy.x, (a1.y + fmaf((float)CNT, h, by0)) - pt.jy.y);
-  const float2 e2 = make_float2((a0.z + gz) - pt.jz.x, (a1.z + gz) - pt.jz.y);
+  const float2 e0 = __fadd2_rn(make_float2(a0.x, a1.x), o.cx);
+  const float2 e1 = __fadd2_rn(make_float2(a0.y, a1.y), __ffma2_rn(make_float2(0.0f, (float)CNT), bcast2(h), o.cy));
+  const float2 e2 = __fadd2_rn(make_float2(a0.z, a1.z), o.cz);
   const float2 d0 = make_float2(b0.x - pt.ux.x, b1.x - pt.ux.y), d1 = make_float2(b0.y - pt.uy.x, b1.y - pt.uy.y);
   const float2 d2 = make_float2(b0.z - pt.uz.x, b1.z - pt.uz.y);
   const float2 v = make_float2((bits[0] & 1u) ? a0.w : 0.0f, ((bits[1] >> CNT) & 1u) ? a1.w : 0.0f);
@@ -396,19 +408,19 @@ __device__ __forceinline__ void deform_pair_ends(const StepParams &p, I j0, I j1
 }
 
 template <int CNT, bool DAMAGE, typename I>
-__device__ __forceinline__ void deform_pair_window(const StepParams &p, int cnt, I jb, I nz, I n, float gx, float gz,
-                                                   float by0, float h, const DeformPair &pt,
+__device__ __forceinline__ void deform_pair_window(const StepParams &p, int cnt, I jb, I nz, I n,
+                                                   const GroupOffsets &o, float h, const DeformPair &pt,
                                                    const uint32_t (&bits)[2], const uint32_t (&live)[2],
                                                    float2 (&part)[9], uint32_t (&fresh)[2], uint32_t (&near)[2]) {
   if constexpr (CNT > 0) {
 #pragma unroll
     for (int t = 1; t < CNT; ++t)  // positions that hold a slot of both points (unclamped: halo)
-      deform_pair_element<DAMAGE, I>(p, t, jb + (I)t * nz, gx, gz, by0, h, pt, bits, live, part, fresh, near);
-    deform_pair_ends<CNT, DAMAGE, I>(p, jb, jb + (I)CNT * nz, gx, gz, by0, h, pt, bits, live, part, fresh, near);
+      deform_pair_element<DAMAGE, I>(p, t, jb + (I)t * nz, o, h, pt, bits, live, part, fresh, near);
+    deform_pair_ends<CNT, DAMAGE, I>(p, jb, jb + (I)CNT * nz, o, h, pt, bits, live, part, fresh, near);
   } else {
     for (int t = 0; t < cnt + 1; ++t)
-      deform_pair_element<DAMAGE, I>(p, t, clamp_to<I>(jb + (I)t * nz, n), gx, gz, by0, h, pt, bits, live, part,
-                                     fresh, near);
+      deform_pair_element<DAMAGE, I>(p, t, clamp_to<I>(jb + (I)t * nz, n), o, h, pt, bits, live, part, fresh,
+                                     near);
   }
 }
 
@@ -475,6 +487,7 @@ __global__ void __launch_bounds__(kBondThreads, 2) k_deformation_pair(const __gr
     if (__all_sync(0xffffffffu, (bits[0] | bits[1]) == 0u))
       continue;
     const float gx = (float)gr.x * h, gz = (float)gr.y * h, by0 = (float)gr.z * h;
+    const GroupOffsets o{sub2(bcast2(gx), pt.jx), sub2(bcast2(by0), pt.jy), sub2(bcast2(gz), pt.jz)};
     const int64_t jb = ((int64_t)(x + gr.x) * ny + (yb * 2 + gr.z)) * nz + (z + gr.y);
     uint32_t fresh[2] = {0u, 0u}, near[2] = {0u, 0u};
     if (UNROLL) {
@@ -482,21 +495,18 @@ __global__ void __launch_bounds__(kBondThreads, 2) k_deformation_pair(const __gr
       const int jb32 = (int)jb, nz32 = nz, n32 = (int)n;
 #define VPD_DEFORM_CASE(C)                                                                                   \
   case C:                                                                                                    \
-    deform_pair_window<C, DAMAGE, int>(p, cnt, jb32, nz32, n32, gx, gz, by0, h, pt, bits, live, part, fresh, \
-                                       near);                                                                \
+    deform_pair_window<C, DAMAGE, int>(p, cnt, jb32, nz32, n32, o, h, pt, bits, live, part, fresh, near);  \
     break;
       switch (cnt) {
         VPD_DEFORM_CASE(1) VPD_DEFORM_CASE(2) VPD_DEFORM_CASE(3) VPD_DEFORM_CASE(4)
         VPD_DEFORM_CASE(5) VPD_DEFORM_CASE(6) VPD_DEFORM_CASE(7) VPD_DEFORM_CASE(8)
         VPD_DEFORM_CASE(9) VPD_DEFORM_CASE(10) VPD_DEFORM_CASE(11) VPD_DEFORM_CASE(12)
       default:
-        deform_pair_window<0, DAMAGE, int>(p, cnt, jb32, nz32, n32, gx, gz, by0, h, pt, bits, live, part, fresh,
-                                           near);
+        deform_pair_window<0, DAMAGE, int>(p, cnt, jb32, nz32, n32, o, h, pt, bits, live, part, fresh, near);
       }
 #undef VPD_DEFORM_CASE
     } else {
-      deform_pair_window<0, DAMAGE, int64_t>(p, cnt, jb, (int64_t)nz, n, gx, gz, by0, h, pt, bits, live, part,
-                                             fresh, near);
+      deform_pair_window<0, DAMAGE, int64_t>(p, cnt, jb, (int64_t)nz, n, o, h, pt, bits, live, part, fresh, near);
     }
     if (DAMAGE)
 #pragma unroll
