@@ -32,6 +32,37 @@ __device__ __forceinline__ void kahan_add2(float2 &s, float2 &c, float2 x) {  //
   s = t;
 }
 
+// The FP32 force map of point j as the mixed force kernels gather it: three float4 records
+// (fmapf[j], fmapf[n + j], fmapf[2 n + j]) holding VM = V_j M_j (row r, column c: VM_rc) and
+// R = VM J_j (J_j: the point's jitter, its reference position less its lattice position):
+//   rec0 = (VM_00, VM_10, VM_01, VM_11)   rec1 = (VM_02, VM_12, R_0, R_1)
+//   rec2 = (VM_20, VM_21, VM_22, R_2)
+// A bond term is VM xi = VM (o + J_j - J_i) = VM e + R with e = o - J_i, which depends on the
+// neighbour only through its own record: rows 0 and 1 of it are three paired multiply-adds of
+// the loaded pairs (VM_0c, VM_1c) with e_c on both lanes, plus the pair (R_0, R_1); row 2 is
+// scalar.
+struct FmapRecord {
+  float2 c0, c1, c2, r01;  // (VM_0c, VM_1c) for c = 0, 1, 2; (R_0, R_1)
+  float m20, m21, m22, r2;  // row 2 and R_2
+};
+__device__ __forceinline__ FmapRecord fmap_record(const float4 &a, const float4 &b, const float4 &c) {
+  return {make_float2(a.x, a.y), make_float2(a.z, a.w), make_float2(b.x, b.y), make_float2(b.z, b.w),
+          c.x, c.y, c.z, c.w};
+}
+// VM e + R for bond reference offset e = o - J_i: rows 0 and 1 as a pair, row 2 scalar
+__device__ __forceinline__ float2 fmap_rows01(const FmapRecord &m, float2 e0, float2 e1, float2 e2) {
+  return __ffma2_rn(m.c2, e2, __ffma2_rn(m.c1, e1, __ffma2_rn(m.c0, e0, m.r01)));
+}
+__device__ __forceinline__ float fmap_row2(const FmapRecord &m, float e0, float e1, float e2) {
+  return fmaf(m.m22, e2, fmaf(m.m21, e1, fmaf(m.m20, e0, m.r2)));
+}
+// Row r of VM (the point's own record, for the M_i s_i term)
+__device__ __forceinline__ void fmap_rows(const float4 &a, const float4 &b, const float4 &c, float (&VM)[9]) {
+  VM[0] = a.x, VM[1] = a.z, VM[2] = b.x;
+  VM[3] = a.y, VM[4] = a.w, VM[5] = b.y;
+  VM[6] = c.x, VM[7] = c.y, VM[8] = c.z;
+}
+
 // FP64 bond arithmetic shared by the per-slot (vpd_stencil.cu) and tiled (vpd_tiled64.cu)
 // kernels, every rounding spelled out so both produce the same bits.
 // G += (v d) (x) e for one bond (v: the neighbour's volume, or 0 without a bond).

@@ -183,12 +183,18 @@ __device__ __forceinline__ void material_store(const StepParams &p, int64_t i, c
   const double4 xi = p.xv[i];
   const double vol = xi.w;
   if (p.mixed) {
+    // the records of fmap_record (vpd_bond.cuh): VM = V M and R = VM J in FP32
     const float4 ji = p.jit[i];
-    const float jr[3] = {ji.x, ji.y, ji.z};
+    double VM[9], R[3];
+#pragma unroll
+    for (int c = 0; c < 9; ++c)
+      VM[c] = vol * M[c];
 #pragma unroll
     for (int r = 0; r < 3; ++r)
-      p.fmapf[r * n + i] = make_float4((float)(vol * M[3 * r]), (float)(vol * M[3 * r + 1]),
-                                       (float)(vol * M[3 * r + 2]), jr[r]);
+      R[r] = VM[3 * r] * (double)ji.x + VM[3 * r + 1] * (double)ji.y + VM[3 * r + 2] * (double)ji.z;
+    p.fmapf[i] = make_float4((float)VM[0], (float)VM[3], (float)VM[1], (float)VM[4]);
+    p.fmapf[n + i] = make_float4((float)VM[2], (float)VM[5], (float)R[0], (float)R[1]);
+    p.fmapf[2 * n + i] = make_float4((float)VM[6], (float)VM[7], (float)VM[8], (float)R[2]);
   } else if (p.fmap) {
     const double xr[3] = {xi.x, xi.y, xi.z};
 #pragma unroll

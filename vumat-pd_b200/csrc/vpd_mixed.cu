@@ -4,7 +4,9 @@
 //   jit[i] = (X_i - lattice_i, V_i) as float4, so a bond vector is
 //            xi = (o h) + (jit_j - jit_i) with the slot's lattice offset o h (float, per slot);
 //   uf[i]  = the predicted displacement as float4, written by the integrator;
-//   fmapf[r * n + i] = row r of V_i M_i (force map scaled by volume) with jit_i's component r.
+//   fmapf[i], fmapf[n + i], fmapf[2 n + i] = V_i M_i (force map scaled by volume) and
+//            (V_i M_i) jit_i, so a bond term V_j M_j xi is V_j M_j (o h - jit_i) + (V_j M_j) jit_j
+//            (fmap_record in vpd_bond.cuh).
 // Each 32-slot word is summed in plain FP32 and the word sums are added with Kahan
 // compensation, so the result carries ~1 FP32 ulp of error (relative ~6e-8) rather than the
 // bond count times it. FP64 stays where the update integrates: K^-1, F = I + G K^-1, the
@@ -97,8 +99,8 @@ __global__ void __launch_bounds__(kBondThreads, 3) k_deformation_mixed(StepParam
 }
 
 // f = sum (V_j M_j) xi over intact bonds + M_i s_i with s_i = vxi_i - sum_{broken j} V_j xi.
-// A bond reads the three FP32 force-map records of j (the jitter offset rides in their fourth
-// lane); the bond sum is FP32 with Kahan-folded words, s_i and the M_i term are FP64.
+// A bond reads the three FP32 force-map records of j (VM_j and VM_j jit_j); the bond sum is
+// FP32 with Kahan-folded words, s_i and the M_i term are FP64.
 __global__ void __launch_bounds__(kBondThreads, 3) k_force_mixed(StepParams p) {
   const int64_t n = p.n;
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -125,31 +127,32 @@ __global__ void __launch_bounds__(kBondThreads, 3) k_force_mixed(StepParams p) {
     }
     if (__all_sync(0xffffffffu, m == 0u))
       continue;
-    float f0 = 0, f1 = 0, f2 = 0;
+    float2 f01 = make_float2(0.0f, 0.0f);
+    float f2 = 0.0f;
 #pragma unroll 4
     for (int b = 0; b < 32; ++b) {
       const bool bond = (m >> b) & 1u;
       const int64_t j = clamp_index(ii + __ldg(dl + b), n);  // contiguous across the warp
       const float4 o = __ldg(ol + b);
-      const float4 a = ldgf4(P0 + j), c = ldgf4(P1 + j), d = ldgf4(P2 + j);
-      const float e0 = bond ? o.x + (a.w - ji.x) : 0.0f;
-      const float e1 = bond ? o.y + (c.w - ji.y) : 0.0f;
-      const float e2 = bond ? o.z + (d.w - ji.z) : 0.0f;
-      f0 += a.x * e0 + a.y * e1 + a.z * e2;
-      f1 += c.x * e0 + c.y * e1 + c.z * e2;
-      f2 += d.x * e0 + d.y * e1 + d.z * e2;
+      const FmapRecord r = fmap_record(ldgf4(P0 + j), ldgf4(P1 + j), ldgf4(P2 + j));
+      const float e0 = o.x - ji.x, e1 = o.y - ji.y, e2 = o.z - ji.z;  // xi less the neighbour's jitter
+      if (bond) {
+        f01 = __fadd2_rn(f01, fmap_rows01(r, bcast2(e0), bcast2(e1), bcast2(e2)));
+        f2 += fmap_row2(r, e0, e1, e2);
+      }
     }
-    kahan_add(fs[0], fc[0], f0), kahan_add(fs[1], fc[1], f1), kahan_add(fs[2], fc[2], f2);
+    kahan_add(fs[0], fc[0], f01.x), kahan_add(fs[1], fc[1], f01.y), kahan_add(fs[2], fc[2], f2);
   }
   if (!valid)
     return;
-  const float4 a = P0[i], c = P1[i], d = P2[i];
+  float VM[9];
+  fmap_rows(P0[i], P1[i], P2[i], VM);
   const double4 s = p.vxi[i];
   const double s0 = s.x - c0, s1 = s.y - c1, s2 = s.z - c2;
   const double rv = 1.0 / (double)ji.w;
-  const double f0 = (double)fs[0] + (a.x * s0 + a.y * s1 + a.z * s2) * rv;
-  const double f1 = (double)fs[1] + (c.x * s0 + c.y * s1 + c.z * s2) * rv;
-  const double f2 = (double)fs[2] + (d.x * s0 + d.y * s1 + d.z * s2) * rv;
+  const double f0 = (double)fs[0] + (VM[0] * s0 + VM[1] * s1 + VM[2] * s2) * rv;
+  const double f1 = (double)fs[1] + (VM[3] * s0 + VM[4] * s1 + VM[5] * s2) * rv;
+  const double f2 = (double)fs[2] + (VM[6] * s0 + VM[7] * s1 + VM[8] * s2) * rv;
   p.force[i] = make_double4(f0, f1, f2, 0.0);
 }
 

@@ -89,7 +89,7 @@ struct StepParams {
   float4 *jit;                // (X_i - lattice position, V_i)
   float4 *uf;                 // predicted displacement
   float *Gf;                  // sum V_j (u_j - u_i) (x) xi, 9 floats structure of arrays
-  float4 *fmapf;              // fmapf[r * n + i] = (VM_r0, VM_r1, VM_r2, jit_r) in FP32
+  float4 *fmapf;              // V_i M_i and (V_i M_i) jit_i in FP32: three records (fmap_record)
   float tension2f, compression2f;
   // surrogate material update (VPD_MATERIAL_SURROGATE, vpd_surrogate.cu)
   int surrogate;              // 1: guess + Newton, bisection fallback, instead of the bisection

@@ -200,18 +200,18 @@ template <int P, typename I>
 __device__ __forceinline__ void force_element(const StepParams &p, int t, int cnt, I j, float gx, float gz,
                                               float by0, float h, const ForcePoints<P> &pt,
                                               const uint32_t (&bits)[P], float (&part)[P][3]) {
-  const float4 a = ldgf4(p.fmapf + j), b = ldgf4(p.fmapf + p.n + j), c = ldgf4(p.fmapf + 2 * p.n + j);
-  const float bx = a.w + gx, by = b.w + fmaf((float)t, h, by0), bz = c.w + gz;
+  const FmapRecord r = fmap_record(ldgf4(p.fmapf + j), ldgf4(p.fmapf + p.n + j), ldgf4(p.fmapf + 2 * p.n + j));
+  const float oy = fmaf((float)t, h, by0);
 #pragma unroll
   for (int q = 0; q < P; ++q) {
     if (t < q || t - q >= cnt)  // window position t holds no slot of point q
       continue;
-    const bool bond = bits[q] & (1u << t);
-    const float e0 = bond ? bx - pt.jx[q] : 0.0f, e1 = bond ? by - pt.jy[q] : 0.0f;
-    const float e2 = bond ? bz - pt.jz[q] : 0.0f;
-    part[q][0] += a.x * e0 + a.y * e1 + a.z * e2;
-    part[q][1] += b.x * e0 + b.y * e1 + b.z * e2;
-    part[q][2] += c.x * e0 + c.y * e1 + c.z * e2;
+    if (bits[q] & (1u << t)) {  // VM_j (o - J_q) + R_j, row by row
+      const float e0 = gx - pt.jx[q], e1 = oy - pt.jy[q], e2 = gz - pt.jz[q];
+      part[q][0] += fmaf(r.c2.x, e2, fmaf(r.c1.x, e1, fmaf(r.c0.x, e0, r.r01.x)));
+      part[q][1] += fmaf(r.c2.y, e2, fmaf(r.c1.y, e1, fmaf(r.c0.y, e0, r.r01.y)));
+      part[q][2] += fmap_row2(r, e0, e1, e2);
+    }
   }
 }
 
@@ -317,13 +317,14 @@ __global__ void __launch_bounds__(kBondThreads, 2) k_force_tiled(const __grid_co
     if (!vp[q])
       continue;
     const int64_t i = ip[q];
-    const float4 a = P0[i], b = P1[i], c = P2[i], ji = p.jit[i];
+    float VM[9];
+    fmap_rows(P0[i], P1[i], P2[i], VM);
     const double4 s = p.vxi[i];
     const double s0 = s.x - corr[q][0], s1 = s.y - corr[q][1], s2 = s.z - corr[q][2];
-    const double rv = 1.0 / (double)ji.w;
-    const double f0 = (double)fs[q][0] + (a.x * s0 + a.y * s1 + a.z * s2) * rv;
-    const double f1 = (double)fs[q][1] + (b.x * s0 + b.y * s1 + b.z * s2) * rv;
-    const double f2 = (double)fs[q][2] + (c.x * s0 + c.y * s1 + c.z * s2) * rv;
+    const double rv = 1.0 / (double)p.jit[i].w;
+    const double f0 = (double)fs[q][0] + (VM[0] * s0 + VM[1] * s1 + VM[2] * s2) * rv;
+    const double f1 = (double)fs[q][1] + (VM[3] * s0 + VM[4] * s1 + VM[5] * s2) * rv;
+    const double f2 = (double)fs[q][2] + (VM[6] * s0 + VM[7] * s1 + VM[8] * s2) * rv;
     p.force[i] = make_double4(f0, f1, f2, 0.0);
   }
 }
@@ -524,69 +525,65 @@ __global__ void __launch_bounds__(kBondThreads, 2) k_deformation_pair(const __gr
   }
 }
 
-struct ForcePair {
-  float2 jx, jy, jz;  // lane q: point q (jy includes q h)
+// The packed force kernel pairs the rows of a neighbour's force map, not the thread's points:
+// a neighbour's records load as the pairs (VM_0c, VM_1c) and (R_0, R_1) (fmap_record), so rows 0
+// and 1 of a bond term are three paired multiply-adds with the point's reference offset on both
+// lanes, and row 2 is three scalar ones; no neighbour value is copied to both lanes of a pair.
+// Point q's offsets from the group's window position 0, o - J_q, on both lanes of a pair
+// (ey at window position t adds t h):
+struct ForceOffsets {
+  float2 ex[2], ey[2], ez[2];
 };
 
-template <typename I>
-__device__ __forceinline__ void force_pair_element(const StepParams &p, int t, I j, float gx, float gz, float by0,
-                                                   float h, const ForcePair &pt, const uint32_t (&bits)[2],
-                                                   float2 (&part)[3]) {
-  const float4 a = ldgf4(p.fmapf + j), b = ldgf4(p.fmapf + p.n + j), c = ldgf4(p.fmapf + 2 * p.n + j);
-  const float bx = a.w + gx, by = b.w + fmaf((float)t, h, by0), bz = c.w + gz;
-  const float2 e0 = sub2(bcast2(bx), pt.jx), e1 = sub2(bcast2(by), pt.jy), e2 = sub2(bcast2(bz), pt.jz);
-  // the row sums of V_j M_j xi, added to the lanes whose point has a bond at position t
-  const float2 m = make_float2(((bits[0] >> t) & 1u) ? 1.0f : 0.0f, ((bits[1] >> t) & 1u) ? 1.0f : 0.0f);
-  const float2 r0 = __ffma2_rn(bcast2(a.z), e2, __ffma2_rn(bcast2(a.y), e1, __fmul2_rn(bcast2(a.x), e0)));
-  const float2 r1 = __ffma2_rn(bcast2(b.z), e2, __ffma2_rn(bcast2(b.y), e1, __fmul2_rn(bcast2(b.x), e0)));
-  const float2 r2 = __ffma2_rn(bcast2(c.z), e2, __ffma2_rn(bcast2(c.y), e1, __fmul2_rn(bcast2(c.x), e0)));
-  part[0] = __ffma2_rn(m, r0, part[0]), part[1] = __ffma2_rn(m, r1, part[1]);
-  part[2] = __ffma2_rn(m, r2, part[2]);
+// Point Q's bond at window position t (if its bit is set): rows 0, 1 into part01, row 2 into part2.
+template <int Q>
+__device__ __forceinline__ void force_pair_point(const FmapRecord &r, int t, float2 th, const ForceOffsets &o,
+                                                 const uint32_t (&bits)[2], float2 (&part01)[2],
+                                                 float (&part2)[2]) {
+  const float2 ey = __fadd2_rn(o.ey[Q], th);
+  const float2 v01 = fmap_rows01(r, o.ex[Q], ey, o.ez[Q]);
+  const float v2 = fmap_row2(r, o.ex[Q].x, ey.x, o.ez[Q].x);
+  if ((bits[Q] >> t) & 1u) {
+    part01[Q] = __fadd2_rn(part01[Q], v01);
+    part2[Q] += v2;
+  }
 }
 
-// The two ends of a window as one pair (lane 0: position 0, lane 1: position CNT), with the
-// operations of force_pair_element.
-template <int CNT, typename I>
-__device__ __forceinline__ void force_pair_ends(const StepParams &p, I j0, I j1, float gx, float gz, float by0,
-                                                float h, const ForcePair &pt, const uint32_t (&bits)[2],
-                                                float2 (&part)[3]) {
-  const float4 *P0 = p.fmapf, *P1 = p.fmapf + p.n, *P2 = p.fmapf + 2 * p.n;
-  const float4 a0 = ldgf4(P0 + j0), b0 = ldgf4(P1 + j0), c0 = ldgf4(P2 + j0);
-  const float4 a1 = ldgf4(P0 + j1), b1 = ldgf4(P1 + j1), c1 = ldgf4(P2 + j1);
-  const float2 e0 = make_float2((a0.w + gx) - pt.jx.x, (a1.w + gx) - pt.jx.y);
-  const float2 e1 = make_float2((b0.w + fmaf(0.0f, h, by0)) - pt.jy.x, (b1.w + fmaf((float)CNT, h, by0)) - pt.jy.y);
-  const float2 e2 = make_float2((c0.w + gz) - pt.jz.x, (c1.w + gz) - pt.jz.y);
-  const float2 m = make_float2((bits[0] & 1u) ? 1.0f : 0.0f, ((bits[1] >> CNT) & 1u) ? 1.0f : 0.0f);
-  const float2 r0 = __ffma2_rn(make_float2(a0.z, a1.z), e2,
-                               __ffma2_rn(make_float2(a0.y, a1.y), e1, __fmul2_rn(make_float2(a0.x, a1.x), e0)));
-  const float2 r1 = __ffma2_rn(make_float2(b0.z, b1.z), e2,
-                               __ffma2_rn(make_float2(b0.y, b1.y), e1, __fmul2_rn(make_float2(b0.x, b1.x), e0)));
-  const float2 r2 = __ffma2_rn(make_float2(c0.z, c1.z), e2,
-                               __ffma2_rn(make_float2(c0.y, c1.y), e1, __fmul2_rn(make_float2(c0.x, c1.x), e0)));
-  part[0] = __ffma2_rn(m, r0, part[0]), part[1] = __ffma2_rn(m, r1, part[1]);
-  part[2] = __ffma2_rn(m, r2, part[2]);
+// Window position t: the neighbour record and its bonds to the points whose slots it holds
+// (Q < 0: both, else point Q only).
+template <int Q, typename I>
+__device__ __forceinline__ void force_pair_element(const StepParams &p, int t, I j, float h, const ForceOffsets &o,
+                                                   const uint32_t (&bits)[2], float2 (&part01)[2],
+                                                   float (&part2)[2]) {
+  const FmapRecord r = fmap_record(ldgf4(p.fmapf + j), ldgf4(p.fmapf + p.n + j), ldgf4(p.fmapf + 2 * p.n + j));
+  const float2 th = bcast2((float)t * h);
+  if (Q <= 0)
+    force_pair_point<0>(r, t, th, o, bits, part01, part2);
+  if (Q != 0)
+    force_pair_point<1>(r, t, th, o, bits, part01, part2);
 }
 
 template <int CNT, typename I>
-__device__ __forceinline__ void force_pair_window(const StepParams &p, int cnt, I jb, I nz, I n, float gx, float gz,
-                                                  float by0, float h, const ForcePair &pt, const uint32_t (&bits)[2],
-                                                  float2 (&part)[3]) {
-  if constexpr (CNT > 0) {
+__device__ __forceinline__ void force_pair_window(const StepParams &p, int cnt, I jb, I nz, I n, float h,
+                                                  const ForceOffsets &o, const uint32_t (&bits)[2],
+                                                  float2 (&part01)[2], float (&part2)[2]) {
+  if constexpr (CNT > 0) {  // unclamped: the records carry zero halos
+    force_pair_element<0, I>(p, 0, jb, h, o, bits, part01, part2);  // point 0's first slot
 #pragma unroll
-    for (int t = 1; t < CNT; ++t)  // positions that hold a slot of both points (unclamped: halo)
-      force_pair_element<I>(p, t, jb + (I)t * nz, gx, gz, by0, h, pt, bits, part);
-    force_pair_ends<CNT, I>(p, jb, jb + (I)CNT * nz, gx, gz, by0, h, pt, bits, part);
+    for (int t = 1; t < CNT; ++t)  // positions that hold a slot of both points
+      force_pair_element<-1, I>(p, t, jb + (I)t * nz, h, o, bits, part01, part2);
+    force_pair_element<1, I>(p, CNT, jb + (I)CNT * nz, h, o, bits, part01, part2);  // point 1's last
   } else {
-    for (int t = 0; t < cnt + 1; ++t)
-      force_pair_element<I>(p, t, clamp_to<I>(jb + (I)t * nz, n), gx, gz, by0, h, pt, bits, part);
+    for (int t = 0; t < cnt + 1; ++t)  // the bits are clear where a position holds no slot of a point
+      force_pair_element<-1, I>(p, t, clamp_to<I>(jb + (I)t * nz, n), h, o, bits, part01, part2);
   }
 }
 
 // f = sum (V_j M_j) xi over intact bonds + M_i s_i with s_i = vxi_i - sum_{broken j} V_j xi.
-// Three blocks per SM (85 registers, a few bytes of spills): the gathers' latency wants the
-// warps more than the unrolled windows want registers (6 % faster than at two blocks on the
-// 1M-point bar; 8 % with damage).
-template <bool UNROLL>
+// Three blocks per SM (85 registers): the gathers' latency wants the warps more than the
+// unrolled windows want registers (6 % faster than at two blocks on the 1M-point bar; 8 % with
+// damage).
+template <bool DAMAGE, bool UNROLL>
 __global__ void __launch_bounds__(kBondThreads, 3) k_force_pair(const __grid_constant__ StepParams p) {
   const int64_t n = p.n;
   const int ny = p.lat_ny, nz = p.lat_nz;
@@ -596,27 +593,29 @@ __global__ void __launch_bounds__(kBondThreads, 3) k_force_pair(const __grid_con
   const float4 *P0 = p.fmapf, *P1 = p.fmapf + n, *P2 = p.fmapf + 2 * n;
   int64_t ip[2];
   bool vp[2];
-  float4 pa[2];
+  float jx[2], jy[2], jz[2];  // jy includes q h (y relative to the thread's first point)
 #pragma unroll
   for (int q = 0; q < 2; ++q) {
     const int y = yb * 2 + q;
     vp[q] = inb && y < ny;
     ip[q] = vp[q] ? ((int64_t)x * ny + y) * nz + z : 0;
-    pa[q] = ldgf4(p.jit + ip[q]);
+    const float4 a = ldgf4(p.jit + ip[q]);
+    jx[q] = a.x, jy[q] = a.y + (float)q * h, jz[q] = a.z;
   }
-  ForcePair pt;
-  pt.jx = make_float2(pa[0].x, pa[1].x), pt.jy = make_float2(pa[0].y, pa[1].y + h);
-  pt.jz = make_float2(pa[0].z, pa[1].z);
-  float2 fs[3], fc[3];
+  // the windows of one stencil plane sum into part01/part2, folded into fs01/fs2 with Kahan
+  // compensation (fc01/fc2)
+  float2 fs01[2], fc01[2], part01[2];
+  float fs2[2], fc2[2], part2[2];
   double corr[2][3];
 #pragma unroll
-  for (int c = 0; c < 3; ++c)
-    fs[c] = fc[c] = make_float2(0.0f, 0.0f), corr[0][c] = corr[1][c] = 0.0;
+  for (int q = 0; q < 2; ++q) {
+    fs01[q] = fc01[q] = part01[q] = make_float2(0.0f, 0.0f);
+    fs2[q] = fc2[q] = part2[q] = 0.0f;
+    corr[q][0] = corr[q][1] = corr[q][2] = 0.0;
+  }
   int word = -1;  // the mask word held in mw (groups come in slot order: several per word)
   int plane = INT_MIN;
   uint32_t mw[2] = {0u, 0u};
-  // the windows of one stencil plane sum into `part`, folded into fs with Kahan compensation
-  float2 part[3] = {make_float2(0.0f, 0.0f), make_float2(0.0f, 0.0f), make_float2(0.0f, 0.0f)};
   for (int g = 0; g < p.st.ngroups; ++g) {
     const int4 gr = __ldg(p.st.groups + g);
     const int cnt = gr.w >> 16, pos = gr.w & 0xffff, wd = pos >> 5, sh = pos & 31;
@@ -624,8 +623,10 @@ __global__ void __launch_bounds__(kBondThreads, 3) k_force_pair(const __grid_con
     if (gr.x != plane) {  // uniform: a new plane
       plane = gr.x;
 #pragma unroll
-      for (int c = 0; c < 3; ++c)
-        kahan_add2(fs[c], fc[c], part[c]), part[c] = make_float2(0.0f, 0.0f);
+      for (int q = 0; q < 2; ++q) {
+        kahan_add2(fs01[q], fc01[q], part01[q]), kahan_add(fs2[q], fc2[q], part2[q]);
+        part01[q] = make_float2(0.0f, 0.0f), part2[q] = 0.0f;
+      }
     }
     if (wd != word) {  // uniform: the group table is the same for every thread
       word = wd;
@@ -637,7 +638,7 @@ __global__ void __launch_bounds__(kBondThreads, 3) k_force_pair(const __grid_con
 #pragma unroll
     for (int q = 0; q < 2; ++q) {
       uint32_t m = group_bits(mw[q], sh, cm);
-      if (p.damage && m) {
+      if (DAMAGE && m) {
         const uint32_t bk = m & group_bits(p.st.broken[(int64_t)wd * n + ip[q]], sh, cm);
         for (uint32_t f = bk; f; f &= f - 1) {  // broken bonds leave s_i
           const int sl = pos + __ffs(f) - 1;
@@ -654,42 +655,44 @@ __global__ void __launch_bounds__(kBondThreads, 3) k_force_pair(const __grid_con
     if (__all_sync(0xffffffffu, (bits[0] | bits[1]) == 0u))
       continue;
     const float gx = (float)gr.x * h, gz = (float)gr.y * h, by0 = (float)gr.z * h;
+    ForceOffsets o;
+#pragma unroll
+    for (int q = 0; q < 2; ++q)
+      o.ex[q] = bcast2(gx - jx[q]), o.ey[q] = bcast2(by0 - jy[q]), o.ez[q] = bcast2(gz - jz[q]);
     const int64_t jb = ((int64_t)(x + gr.x) * ny + (yb * 2 + gr.z)) * nz + (z + gr.y);
     if (UNROLL) {
       static_assert(kUnrolledSlots == 12, "the cases below list the unrolled slot counts");
       const int jb32 = (int)jb, nz32 = nz, n32 = (int)n;
 #define VPD_FORCE_CASE(C)                                                                 \
   case C:                                                                                 \
-    force_pair_window<C, int>(p, cnt, jb32, nz32, n32, gx, gz, by0, h, pt, bits, part);   \
+    force_pair_window<C, int>(p, cnt, jb32, nz32, n32, h, o, bits, part01, part2);        \
     break;
       switch (cnt) {
         VPD_FORCE_CASE(1) VPD_FORCE_CASE(2) VPD_FORCE_CASE(3) VPD_FORCE_CASE(4)
         VPD_FORCE_CASE(5) VPD_FORCE_CASE(6) VPD_FORCE_CASE(7) VPD_FORCE_CASE(8)
         VPD_FORCE_CASE(9) VPD_FORCE_CASE(10) VPD_FORCE_CASE(11) VPD_FORCE_CASE(12)
       default:
-        force_pair_window<0, int>(p, cnt, jb32, nz32, n32, gx, gz, by0, h, pt, bits, part);
+        force_pair_window<0, int>(p, cnt, jb32, nz32, n32, h, o, bits, part01, part2);
       }
 #undef VPD_FORCE_CASE
     } else {
-      force_pair_window<0, int64_t>(p, cnt, jb, (int64_t)nz, n, gx, gz, by0, h, pt, bits, part);
+      force_pair_window<0, int64_t>(p, cnt, jb, (int64_t)nz, n, h, o, bits, part01, part2);
     }
   }
 #pragma unroll
-  for (int c = 0; c < 3; ++c)
-    kahan_add2(fs[c], fc[c], part[c]);
-#pragma unroll
   for (int q = 0; q < 2; ++q) {
+    kahan_add2(fs01[q], fc01[q], part01[q]), kahan_add(fs2[q], fc2[q], part2[q]);
     if (!vp[q])
       continue;
     const int64_t i = ip[q];
-    const float4 a = P0[i], b = P1[i], c = P2[i], ji = p.jit[i];
+    float VM[9];
+    fmap_rows(P0[i], P1[i], P2[i], VM);
     const double4 s = p.vxi[i];
     const double s0 = s.x - corr[q][0], s1 = s.y - corr[q][1], s2 = s.z - corr[q][2];
-    const double rv = 1.0 / (double)ji.w;
-    const float f0s = q ? fs[0].y : fs[0].x, f1s = q ? fs[1].y : fs[1].x, f2s = q ? fs[2].y : fs[2].x;
-    const double f0 = (double)f0s + (a.x * s0 + a.y * s1 + a.z * s2) * rv;
-    const double f1 = (double)f1s + (b.x * s0 + b.y * s1 + b.z * s2) * rv;
-    const double f2 = (double)f2s + (c.x * s0 + c.y * s1 + c.z * s2) * rv;
+    const double rv = 1.0 / (double)p.jit[i].w;
+    const double f0 = (double)fs01[q].x + (VM[0] * s0 + VM[1] * s1 + VM[2] * s2) * rv;
+    const double f1 = (double)fs01[q].y + (VM[3] * s0 + VM[4] * s1 + VM[5] * s2) * rv;
+    const double f2 = (double)fs2[q] + (VM[6] * s0 + VM[7] * s1 + VM[8] * s2) * rv;
     p.force[i] = make_double4(f0, f1, f2, 0.0);
   }
 }
@@ -730,10 +733,12 @@ int launch_force_tiled(const StepParams &p, cudaStream_t s) {
     else
       k_force_tiled<2, false><<<grid, kBondThreads, 0, s>>>(p);
   } else {
-    if (u)
-      k_force_pair<true><<<grid, kBondThreads, 0, s>>>(p);
+    if (p.damage)
+      u ? k_force_pair<true, true><<<grid, kBondThreads, 0, s>>>(p)
+        : k_force_pair<true, false><<<grid, kBondThreads, 0, s>>>(p);
     else
-      k_force_pair<false><<<grid, kBondThreads, 0, s>>>(p);
+      u ? k_force_pair<false, true><<<grid, kBondThreads, 0, s>>>(p)
+        : k_force_pair<false, false><<<grid, kBondThreads, 0, s>>>(p);
   }
   VPD_CUDA(cudaGetLastError());
   return VPD_OK;
