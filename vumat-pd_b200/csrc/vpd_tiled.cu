@@ -580,11 +580,10 @@ __device__ __forceinline__ void force_pair_window(const StepParams &p, int cnt, 
 }
 
 // f = sum (V_j M_j) xi over intact bonds + M_i s_i with s_i = vxi_i - sum_{broken j} V_j xi.
-// Three blocks per SM (85 registers): the gathers' latency wants the warps more than the
-// unrolled windows want registers (6 % faster than at two blocks on the 1M-point bar; 8 % with
-// damage).
+// Two blocks per SM (128 registers, no spills): 0.375 against 0.393 ms at three blocks (80
+// registers and spills) on the 1M-point bar in plastic flow.
 template <bool DAMAGE, bool UNROLL>
-__global__ void __launch_bounds__(kBondThreads, 3) k_force_pair(const __grid_constant__ StepParams p) {
+__global__ void __launch_bounds__(kBondThreads, 2) k_force_pair(const __grid_constant__ StepParams p) {
   const int64_t n = p.n;
   const int ny = p.lat_ny, nz = p.lat_nz;
   const float h = (float)p.lat_h;
