@@ -48,6 +48,39 @@ __device__ __forceinline__ void stretch_test(const StepParams &p, int t, float e
   }
 }
 
+// The stretch-test decision of one bond from yy = |y|^2, xx = |xi|^2 and the tension bounds
+// thi = tension2f xx (1 + 1e-5), tlo = tension2f xx (1 - 1e-5) (stretch_test's comparisons),
+// without branches: bit t of fresh / near set where the bond at t is live (l).
+__device__ __forceinline__ void stretch_classify(const StepParams &p, int t, bool l, float yy, float xx, float thi,
+                                                 float tlo, uint32_t &fresh, uint32_t &near) {
+  bool f = yy > thi, r = !f && yy >= tlo;
+  if (p.use_compression) {  // uniform
+    const float c = p.compression2f * xx;
+    const bool cf = yy < c * (1.0f - 1.0e-5f), cr = yy <= c * (1.0f + 1.0e-5f);
+    r = r || (!f && !r && !cf && cr);
+    f = f || (!r && cf);
+  }
+  fresh |= (uint32_t)(l && f) << t;
+  near |= (uint32_t)(l && r) << t;
+}
+
+// The stretch tests of the two lanes of a packed element, paired: lane q holds a bond at window
+// position tq, tested when bit tq of live[q] is set (the arithmetic of stretch_test per lane).
+__device__ __forceinline__ void stretch_test2(const StepParams &p, int t0, int t1, float2 e0, float2 e1, float2 e2,
+                                              float2 d0, float2 d1, float2 d2, const uint32_t (&live)[2],
+                                              uint32_t (&fresh)[2], uint32_t (&near)[2]) {
+  const bool l0 = (live[0] >> t0) & 1u, l1 = (live[1] >> t1) & 1u;
+  if (!(l0 || l1))
+    return;
+  const float2 y0 = __fadd2_rn(e0, d0), y1 = __fadd2_rn(e1, d1), y2 = __fadd2_rn(e2, d2);
+  const float2 yy = __ffma2_rn(y2, y2, __ffma2_rn(y1, y1, __fmul2_rn(y0, y0)));
+  const float2 xx = __ffma2_rn(e2, e2, __ffma2_rn(e1, e1, __fmul2_rn(e0, e0)));
+  const float2 tt = __fmul2_rn(bcast2(p.tension2f), xx);
+  const float2 thi = __fmul2_rn(tt, bcast2(1.0f + 1.0e-5f)), tlo = __fmul2_rn(tt, bcast2(1.0f - 1.0e-5f));
+  stretch_classify(p, t0, l0, yy.x, xx.x, thi.x, tlo.x, fresh[0], near[0]);
+  stretch_classify(p, t1, l1, yy.y, xx.y, thi.y, tlo.y, fresh[1], near[1]);
+}
+
 // ------------------------------------------------------------------ deformation
 template <int P> struct DeformPoints {
   float jx[P], jy[P], jz[P], ux[P], uy[P], uz[P];  // jy includes q h (y relative to the tile's base row)
@@ -371,12 +404,8 @@ __device__ __forceinline__ void deform_pair_element(const StepParams &p, int t, 
   part[4] = __ffma2_rn(w1, e1, part[4]), part[5] = __ffma2_rn(w1, e2, part[5]);
   part[6] = __ffma2_rn(w2, e0, part[6]), part[7] = __ffma2_rn(w2, e1, part[7]);
   part[8] = __ffma2_rn(w2, e2, part[8]);
-  if (DAMAGE) {
-    if ((live[0] >> t) & 1u)
-      stretch_test(p, t, e0.x, e1.x, e2.x, d0.x, d1.x, d2.x, fresh[0], near[0]);
-    if ((live[1] >> t) & 1u)
-      stretch_test(p, t, e0.y, e1.y, e2.y, d0.y, d1.y, d2.y, fresh[1], near[1]);
-  }
+  if (DAMAGE)
+    stretch_test2(p, t, t, e0, e1, e2, d0, d1, d2, live, fresh, near);
 }
 
 // The two ends of a window of CNT slots as one pair: lane 0 takes position 0 (point 0's first
@@ -400,12 +429,8 @@ __device__ __forceinline__ void deform_pair_ends(const StepParams &p, I j0, I j1
   part[4] = __ffma2_rn(w1, e1, part[4]), part[5] = __ffma2_rn(w1, e2, part[5]);
   part[6] = __ffma2_rn(w2, e0, part[6]), part[7] = __ffma2_rn(w2, e1, part[7]);
   part[8] = __ffma2_rn(w2, e2, part[8]);
-  if (DAMAGE) {
-    if (live[0] & 1u)
-      stretch_test(p, 0, e0.x, e1.x, e2.x, d0.x, d1.x, d2.x, fresh[0], near[0]);
-    if ((live[1] >> CNT) & 1u)
-      stretch_test(p, CNT, e0.y, e1.y, e2.y, d0.y, d1.y, d2.y, fresh[1], near[1]);
-  }
+  if (DAMAGE)
+    stretch_test2(p, 0, CNT, e0, e1, e2, d0, d1, d2, live, fresh, near);
 }
 
 template <int CNT, bool DAMAGE, typename I>
@@ -456,7 +481,9 @@ __global__ void __launch_bounds__(kBondThreads, 2) k_deformation_pair(const __gr
     G[c] = Gc[c] = part[c] = make_float2(0.0f, 0.0f);
   int word = -1;  // the mask word held in mw (groups come in slot order: several per word)
   int plane = INT_MIN;
-  uint32_t mw[2] = {0u, 0u};
+  // mw: the mask words; bw: the broken-bond words, read with them (only this thread sets the
+  // bits of its points' forward slots, the only ones tested, and each slot is in one group)
+  uint32_t mw[2] = {0u, 0u}, bw[2] = {0u, 0u};
   for (int g = 0; g < p.st.ngroups; ++g) {
     const int4 gr = __ldg(p.st.groups + g);  // dx, dz, lowest dy, (slots << 16) | first slot
     const int cnt = gr.w >> 16, pos = gr.w & 0xffff, wd = pos >> 5, sh = pos & 31;
@@ -470,8 +497,11 @@ __global__ void __launch_bounds__(kBondThreads, 2) k_deformation_pair(const __gr
     if (wd != word) {  // uniform: the group table is the same for every thread
       word = wd;
 #pragma unroll
-      for (int q = 0; q < 2; ++q)
+      for (int q = 0; q < 2; ++q) {
         mw[q] = vp[q] ? __ldg(p.st.mask + (int64_t)wd * n + ip[q]) : 0u;
+        if (DAMAGE)
+          bw[q] = vp[q] ? p.st.broken[(int64_t)wd * n + ip[q]] : 0u;
+      }
     }
     uint32_t bits[2], live[2];
     const uint32_t fw = DAMAGE ? group_bits(__ldg(p.st.forward + wd), sh, cm) : 0u;
@@ -479,11 +509,7 @@ __global__ void __launch_bounds__(kBondThreads, 2) k_deformation_pair(const __gr
     for (int q = 0; q < 2; ++q) {
       const uint32_t m = group_bits(mw[q], sh, cm);
       bits[q] = m << q;  // bit t: the neighbour at window position t (slot pos + t - q)
-      live[q] = 0u;
-      if (DAMAGE) {
-        const uint32_t bk = vp[q] ? group_bits(p.st.broken[(int64_t)wd * n + ip[q]], sh, cm) : 0u;
-        live[q] = (m & fw & ~bk) << q;
-      }
+      live[q] = DAMAGE ? (m & fw & ~group_bits(bw[q], sh, cm)) << q : 0u;
     }
     if (__all_sync(0xffffffffu, (bits[0] | bits[1]) == 0u))
       continue;
@@ -612,9 +638,9 @@ __global__ void __launch_bounds__(kBondThreads, 2) k_force_pair(const __grid_con
     fs2[q] = fc2[q] = part2[q] = 0.0f;
     corr[q][0] = corr[q][1] = corr[q][2] = 0.0;
   }
-  int word = -1;  // the mask word held in mw (groups come in slot order: several per word)
+  int word = -1;  // the mask (and broken-bond) words held in mw (bw): several groups per word
   int plane = INT_MIN;
-  uint32_t mw[2] = {0u, 0u};
+  uint32_t mw[2] = {0u, 0u}, bw[2] = {0u, 0u};
   for (int g = 0; g < p.st.ngroups; ++g) {
     const int4 gr = __ldg(p.st.groups + g);
     const int cnt = gr.w >> 16, pos = gr.w & 0xffff, wd = pos >> 5, sh = pos & 31;
@@ -630,15 +656,18 @@ __global__ void __launch_bounds__(kBondThreads, 2) k_force_pair(const __grid_con
     if (wd != word) {  // uniform: the group table is the same for every thread
       word = wd;
 #pragma unroll
-      for (int q = 0; q < 2; ++q)
+      for (int q = 0; q < 2; ++q) {
         mw[q] = vp[q] ? __ldg(p.st.mask + (int64_t)wd * n + ip[q]) : 0u;
+        if (DAMAGE)  // written by the deformation kernel, read-only here
+          bw[q] = vp[q] ? __ldg(p.st.broken + (int64_t)wd * n + ip[q]) : 0u;
+      }
     }
     uint32_t bits[2];
 #pragma unroll
     for (int q = 0; q < 2; ++q) {
       uint32_t m = group_bits(mw[q], sh, cm);
       if (DAMAGE && m) {
-        const uint32_t bk = m & group_bits(p.st.broken[(int64_t)wd * n + ip[q]], sh, cm);
+        const uint32_t bk = m & group_bits(bw[q], sh, cm);
         for (uint32_t f = bk; f; f &= f - 1) {  // broken bonds leave s_i
           const int sl = pos + __ffs(f) - 1;
           const float4 jj = p.jit[ip[q] + p.st.delta[sl]], o = p.st.e0[sl];
