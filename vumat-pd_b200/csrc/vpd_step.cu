@@ -309,8 +309,12 @@ __global__ void __launch_bounds__(kBondThreads, 3) k_integrate(StepParams p) {
   const int ngroups = (int)((gridDim.x + kGroupBlocks - 1) / kGroupBlocks);
   const int g = (int)(blockIdx.x / kGroupBlocks), gfirst = g * kGroupBlocks;
   const int gcount = min(kGroupBlocks, (int)gridDim.x - gfirst);
+  // the threads that wrote the block's partials make them visible device-wide, and the barrier
+  // orders that before the block is counted
   __shared__ bool last;
-  __threadfence();
+  if (threadIdx.x < PF_COUNT)
+    __threadfence();
+  __syncthreads();
   if (threadIdx.x == 0)
     last = atomicAdd(p.group_counter + g, 1u) == (unsigned)gcount - 1u;
   __syncthreads();

@@ -728,7 +728,7 @@ __global__ void __launch_bounds__(kBondThreads, 2) k_force_pair(const __grid_con
 // ------------------------------------------------------------------ launchers
 // With damage the scalar deformation kernel keeps the runtime window loop (unrolled, its
 // stretch tests made it slower: 0.28 against 0.25 ms on the 250k-point bar); the packed-pair
-// kernel unrolls its windows with damage too (0.72 against 0.75 ms on the 1M-point bar).
+// kernel unrolls its windows with damage too (0.698 against 0.783 ms on the 1M-point bar).
 template <bool UNROLL> static void launch_deformation(const StepParams &p, cudaStream_t s) {
   const unsigned grid = tiled_grid<2>(p);
   if (p.tiled == 1) {
