@@ -233,6 +233,8 @@ struct vpd_handle {
   uint8_t *flags = nullptr;
   unsigned *status_dev = nullptr, *counter = nullptr;
   double *pdmg = nullptr;      // point damage (point damage modes only)
+  double *field_buf = nullptr;  // device buffer of vpd_download's point-major layouts
+  int64_t field_cap = 0;        // its doubles
   uint16_t *surr_w = nullptr;  // surrogate network (device copies)
   float *surr_b = nullptr;
   bool surrogate_ready = false;
@@ -516,6 +518,7 @@ void destroy_impl(vpd_handle *h) {
   host_vumat_detach(h->params);
   for (void *p : h->allocations)
     cudaFree(p);
+  cudaFree(h->field_buf);
   free_stencil(h->st);
   if (h->ev0)
     cudaEventDestroy(h->ev0);
@@ -634,6 +637,62 @@ CheckpointHeader checkpoint_header(vpd_handle *h, const std::vector<Section> &v)
     hd.payload += sec.bytes;
   hd.c = h->c;
   return hd;
+}
+
+}  // namespace
+
+namespace {
+// Point-major layouts of vpd_download, formed on the device (one copy to the host follows).
+// MODE 0: components 0..comps-1 (or the fourth, comps == 1) of a double4 array; 1: a structure
+// of arrays; 2: a Voigt tensor (11,22,33,23,13,12) as the full 3x3; 3: the spatial stress
+// R sigma R^T from the Voigt corotational stress and R, rounded as the host loop it replaces
+// (separate products and sums, left to right).
+template <int MODE>
+__global__ void k_field_pack(int64_t n, int comps, const double4 *v4, const double *a, const double *b,
+                             double *out) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n)
+    return;
+  if (MODE == 0) {
+    const double4 v = v4[i];
+    if (comps == 1) {
+      out[i] = v.w;
+    } else {
+      out[3 * i] = v.x, out[3 * i + 1] = v.y, out[3 * i + 2] = v.z;
+    }
+  } else if (MODE == 1) {
+    for (int c = 0; c < comps; ++c)
+      out[comps * i + c] = a[c * n + i];
+  } else {
+    double v[6];
+#pragma unroll
+    for (int c = 0; c < 6; ++c)
+      v[c] = a[c * n + i];
+    const double f[9] = {v[0], v[5], v[4], v[5], v[1], v[3], v[4], v[3], v[2]};
+    double *o = out + 9 * i;
+    if (MODE == 2) {
+#pragma unroll
+      for (int c = 0; c < 9; ++c)
+        o[c] = f[c];
+    } else {
+      double R[9], t[9];
+#pragma unroll
+      for (int c = 0; c < 9; ++c)
+        R[c] = b[c * n + i];
+#pragma unroll
+      for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+          t[3 * r + c] = __dadd_rn(__dadd_rn(__dmul_rn(f[3 * r], R[3 * c]), __dmul_rn(f[3 * r + 1], R[3 * c + 1])),
+                                   __dmul_rn(f[3 * r + 2], R[3 * c + 2]));
+#pragma unroll
+      for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+          o[3 * r + c] = __dadd_rn(__dadd_rn(__dmul_rn(R[3 * r], t[c]), __dmul_rn(R[3 * r + 1], t[3 + c])),
+                                   __dmul_rn(R[3 * r + 2], t[6 + c]));
+    }
+  }
 }
 
 }  // namespace
@@ -936,19 +995,25 @@ int vpd_download(vpd_handle *h, int32_t field, double *out) {
     return set_error(VPD_ERR_INVALID, "NULL argument");
   const int64_t n = h->n;
   cudaStream_t s = h->stream;
-  auto get4 = [&](const double4 *src, int comps) -> int {
-    std::vector<double4> buf((size_t)n);
-    VPD_CUDA(cudaMemcpyAsync(buf.data(), src, sizeof(double4) * n, cudaMemcpyDeviceToHost, s));
-    VPD_CUDA(cudaStreamSynchronize(s));
-    for (int64_t i = 0; i < n; ++i) {
-      const double v[4] = {buf[i].x, buf[i].y, buf[i].z, buf[i].w};
-      if (comps == 1)
-        out[i] = v[3];
-      else
-        for (int d = 0; d < 3; ++d)
-          out[3 * i + d] = v[d];
+  // a point-major field of `comps` doubles per point packed by k_field_pack<MODE> into the
+  // handle's device buffer, then one copy into the caller's array
+  auto packed = [&](auto kernel, int comps, const double4 *v4, const double *a, const double *b) -> int {
+    const int64_t need = (int64_t)comps * n;
+    if (need > h->field_cap) {  // sized once for the widest field
+      cudaFree(h->field_buf);
+      h->field_buf = nullptr, h->field_cap = 0;
+      const int64_t cap = std::max<int64_t>(need, (int64_t)std::max(9, h->c.nstatev) * n);
+      VPD_CUDA(cudaMalloc(&h->field_buf, sizeof(double) * cap));
+      h->field_cap = cap;
     }
+    kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, comps, v4, a, b, h->field_buf);
+    VPD_CUDA(cudaGetLastError());
+    VPD_CUDA(cudaMemcpyAsync(out, h->field_buf, sizeof(double) * need, cudaMemcpyDeviceToHost, s));
+    VPD_CUDA(cudaStreamSynchronize(s));
     return VPD_OK;
+  };
+  auto get4 = [&](const double4 *src, int comps) -> int {
+    return packed(k_field_pack<0>, comps == 1 ? 1 : 3, src, nullptr, nullptr);
   };
   auto getSoA = [&](const double *src, int comps, std::vector<double> &buf) -> int {
     buf.resize((size_t)(comps * n));
@@ -957,27 +1022,10 @@ int vpd_download(vpd_handle *h, int32_t field, double *out) {
     return VPD_OK;
   };
   auto aos = [&](const double *src, int comps) -> int {
-    std::vector<double> buf;
-    int rc = getSoA(src, comps, buf);
-    if (rc)
-      return rc;
-    for (int64_t i = 0; i < n; ++i)
-      for (int c = 0; c < comps; ++c)
-        out[comps * i + c] = buf[c * n + i];
-    return VPD_OK;
+    return packed(k_field_pack<1>, comps, nullptr, src, nullptr);
   };
   auto sym = [&](const double *src) -> int {  // Voigt 11,22,33,23,13,12 -> full 3x3
-    std::vector<double> buf;
-    int rc = getSoA(src, 6, buf);
-    if (rc)
-      return rc;
-    for (int64_t i = 0; i < n; ++i) {
-      const double v[6] = {buf[i], buf[n + i], buf[2 * n + i], buf[3 * n + i], buf[4 * n + i], buf[5 * n + i]};
-      double *o = out + 9 * i;
-      o[0] = v[0], o[1] = v[5], o[2] = v[4], o[3] = v[5], o[4] = v[1], o[5] = v[3];
-      o[6] = v[4], o[7] = v[3], o[8] = v[2];
-    }
-    return VPD_OK;
+    return packed(k_field_pack<2>, 9, nullptr, src, nullptr);
   };
   switch (field) {
   case VPD_FIELD_POSITION: return get4(h->xv, 3);
@@ -995,26 +1043,8 @@ int vpd_download(vpd_handle *h, int32_t field, double *out) {
   case VPD_FIELD_ENERGY_INELASTIC: return aos(h->eP, 1);
   case VPD_FIELD_STRESS_COROTATIONAL: return sym(h->sig);
   case VPD_FIELD_STRAIN: return sym(h->En);
-  case VPD_FIELD_STRESS_SPATIAL: {
-    std::vector<double> sg, r;
-    int rc;
-    if ((rc = getSoA(h->sig, 6, sg)) || (rc = getSoA(h->Rn, 9, r)))
-      return rc;
-    for (int64_t i = 0; i < n; ++i) {
-      const double v[6] = {sg[i], sg[n + i], sg[2 * n + i], sg[3 * n + i], sg[4 * n + i], sg[5 * n + i]};
-      const double f[9] = {v[0], v[5], v[4], v[5], v[1], v[3], v[4], v[3], v[2]};
-      double R[9], tmp[9];
-      for (int c = 0; c < 9; ++c)
-        R[c] = r[c * n + i];
-      for (int a = 0; a < 3; ++a)
-        for (int b = 0; b < 3; ++b)
-          tmp[3 * a + b] = f[3 * a] * R[3 * b] + f[3 * a + 1] * R[3 * b + 1] + f[3 * a + 2] * R[3 * b + 2];
-      for (int a = 0; a < 3; ++a)
-        for (int b = 0; b < 3; ++b)
-          out[9 * i + 3 * a + b] = R[3 * a] * tmp[b] + R[3 * a + 1] * tmp[3 + b] + R[3 * a + 2] * tmp[6 + b];
-    }
-    return VPD_OK;
-  }
+  case VPD_FIELD_STRESS_SPATIAL:  // R sigma R^T
+    return packed(k_field_pack<3>, 9, nullptr, h->sig, h->Rn);
   case VPD_FIELD_TEMPERATURE: {
     if (h->params.host_vumat) {  // the plugin's tempNew, kept per point
       VPD_CUDA(cudaMemcpyAsync(out, h->params.temp, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
