@@ -10,7 +10,9 @@
 #include "vpd_step.cuh"
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <limits>
 #include <string>
@@ -310,7 +312,30 @@ int read_status(vpd_handle *h) {
   return VPD_OK;
 }
 
+// VPD_TRACE=1: the wall-clock time of each phase of vpd_create (the stream synchronised at every
+// mark) on stderr.
+struct CreateTrace {
+  bool on = false;
+  cudaStream_t stream = nullptr;
+  std::chrono::steady_clock::time_point last = std::chrono::steady_clock::now();
+  CreateTrace() {
+    const char *t = getenv("VPD_TRACE");
+    on = t && t[0] == '1';
+  }
+  void mark(const char *phase) {
+    if (!on)
+      return;
+    if (stream)
+      cudaStreamSynchronize(stream);
+    const auto now = std::chrono::steady_clock::now();
+    fprintf(stderr, "vpd_create %-28s %9.2f ms\n", phase,
+            std::chrono::duration<double, std::milli>(now - last).count());
+    last = now;
+  }
+};
+
 int create_impl(vpd_handle *h, const vpd_case *c, const double *positions, const double *volumes) {
+  CreateTrace trace;
   int rc = check_case(c);
   if (rc)
     return rc;
@@ -341,6 +366,7 @@ int create_impl(vpd_handle *h, const vpd_case *c, const double *positions, const
   Sets sets;
   if ((rc = build_sets(*c, nominal, vol, sets)))
     return rc;
+  trace.mark("host sets");
   VPD_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
   VPD_CUDA(cudaEventCreate(&h->ev0));
   VPD_CUDA(cudaEventCreate(&h->ev1));
@@ -364,6 +390,8 @@ int create_impl(vpd_handle *h, const vpd_case *c, const double *positions, const
       return rc;
     VPD_CUDA(cudaMemsetAsync(h->pdmg, 0, sizeof(double) * n, s));
   }
+  trace.stream = s;
+  trace.mark("device arrays");
   VPD_CUDA(cudaMemsetAsync(h->u0, 0, sizeof(double4) * n, s));
   VPD_CUDA(cudaMemsetAsync(h->status_dev, 0, sizeof(unsigned), s));
   VPD_CUDA(cudaMemsetAsync(h->counter, 0, sizeof(unsigned), s));
@@ -385,6 +413,7 @@ int create_impl(vpd_handle *h, const vpd_case *c, const double *positions, const
                     c->jitter != 0.0};
     k_lattice<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(L, h->xv);
   }
+  trace.mark("positions");
   VPD_CUDA(cudaMemcpyAsync(h->flags, sets.flags.data(), n, cudaMemcpyHostToDevice, s));
   VPD_CUDA(cudaMemcpyAsync(h->obsw, sets.obsw.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s));
 
@@ -403,6 +432,7 @@ int create_impl(vpd_handle *h, const vpd_case *c, const double *positions, const
     if (rc)
       return rc;
   }
+  trace.mark("neighbour lists");
   // the bond layout the kernels stream: lattice-stencil bit masks when the points form the
   // lattice in index order (every generated patch), else the sliced ELL
   // (VPD_BOND_LAYOUT=ell selects the sliced ELL for any case)
@@ -420,6 +450,7 @@ int create_impl(vpd_handle *h, const vpd_case *c, const double *positions, const
       return rc;
     VPD_CUDA(cudaMemsetAsync(h->words, 0, sizeof(uint32_t) * std::max<int64_t>(h->sell_total / 32, 1), s));
   }
+  trace.mark("bond layout");
   const int mat_blocks = material_grid(n);
   const int force_blocks = integrate_grid(n);
   const int groups = (force_blocks + kGroupBlocks - 1) / kGroupBlocks;
@@ -497,6 +528,7 @@ int create_impl(vpd_handle *h, const vpd_case *c, const double *positions, const
   p.area = sets.area, p.n_lat_pos = sets.n_lat_pos, p.n_lat_neg = sets.n_lat_neg;
   p.sign = (c->bc_mode == VPD_BC_SMOOTH_DISPLACEMENT ? c->amplitude : c->grip_velocity) > 0.0 ? 1.0 : -1.0;
 
+  trace.mark("parameters, mixed arrays");
   if ((rc = p.st.nw ? launch_shape_stencil(p, s) : launch_shape_inverse_sell(p, s)))
     return rc;
   if ((rc = launch_init(p, s)))
@@ -507,7 +539,9 @@ int create_impl(vpd_handle *h, const vpd_case *c, const double *positions, const
   const int64_t one = 1;
   VPD_CUDA(cudaMemcpyAsync(h->accum, acc0, sizeof acc0, cudaMemcpyHostToDevice, s));
   VPD_CUDA(cudaMemcpyAsync(h->step_dev, &one, sizeof one, cudaMemcpyHostToDevice, s));
-  return read_status(h);
+  const int status = read_status(h);
+  trace.mark("shape tensors, initial state");
+  return status;
 }
 
 void destroy_impl(vpd_handle *h) {
