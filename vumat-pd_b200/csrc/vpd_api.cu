@@ -421,18 +421,23 @@ int create_impl(vpd_handle *h, const vpd_case *c, const double *positions, const
   {
     NeighborScratch scr;
     NeighborGrid grid;
-    if ((rc = neighbor_scratch_alloc(scr, n)) == VPD_OK &&
-        (rc = neighbor_count(h->xv, n, c->horizon, h->row_ptr, grid, scr, s)) == VPD_OK) {
-      VPD_CUDA(cudaMemcpyAsync(&h->nbonds, h->row_ptr + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
-      VPD_CUDA(cudaStreamSynchronize(s));
-      if ((rc = dalloc(h, &h->col, (size_t)h->nbonds)) == VPD_OK)
-        rc = neighbor_fill(h->xv, n, h->row_ptr, h->col, grid, scr, s);
+    if ((rc = neighbor_scratch_alloc(scr, n)) == VPD_OK) {
+      trace.mark("neighbour scratch");
+      if ((rc = neighbor_count(h->xv, n, c->horizon, h->row_ptr, grid, scr, s)) == VPD_OK) {
+        VPD_CUDA(cudaMemcpyAsync(&h->nbonds, h->row_ptr + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+        VPD_CUDA(cudaStreamSynchronize(s));
+        trace.mark("neighbour count");
+        if ((rc = dalloc(h, &h->col, (size_t)h->nbonds)) == VPD_OK) {
+          trace.mark("neighbour list allocation");
+          rc = neighbor_fill(h->xv, n, h->row_ptr, h->col, grid, scr, s);
+        }
+      }
     }
     neighbor_scratch_free(scr);
     if (rc)
       return rc;
   }
-  trace.mark("neighbour lists");
+  trace.mark("neighbour fill, scratch freed");
   // the bond layout the kernels stream: lattice-stencil bit masks when the points form the
   // lattice in index order (every generated patch), else the sliced ELL
   // (VPD_BOND_LAYOUT=ell selects the sliced ELL for any case)
