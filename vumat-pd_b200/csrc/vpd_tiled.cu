@@ -25,6 +25,10 @@
 
 namespace vpd {
 
+template <bool B> struct BoolConstant {
+  static constexpr bool value = B;
+};
+
 // FP32 critical-stretch test of one live bond (reference xi = e, displacement difference d):
 // bit t of `fresh` when the bond is clearly broken, of `near` when it is within the 1e-5 margin
 // of a threshold and the exact FP64 test decides.
@@ -517,24 +521,34 @@ __global__ void __launch_bounds__(kBondThreads, 2) k_deformation_pair(const __gr
     const GroupOffsets o{sub2(bcast2(gx), pt.jx), sub2(bcast2(by0), pt.jy), sub2(bcast2(gz), pt.jz)};
     const int64_t jb = ((int64_t)(x + gr.x) * ny + (yb * 2 + gr.z)) * nz + (z + gr.y);
     uint32_t fresh[2] = {0u, 0u}, near[2] = {0u, 0u};
-    if (UNROLL) {
-      static_assert(kUnrolledSlots == 12, "the cases below list the unrolled slot counts");
-      const int jb32 = (int)jb, nz32 = nz, n32 = (int)n;
+    // windows with stretch tests only where some lane of the warp has a live bond in the group
+    // (with damage: the forward groups, less their broken bonds)
+    const bool tests = DAMAGE && __any_sync(0xffffffffu, (live[0] | live[1]) != 0u);
+    auto windows = [&](auto tested) {
+      constexpr bool D = decltype(tested)::value;
+      if (UNROLL) {
+        static_assert(kUnrolledSlots == 12, "the cases below list the unrolled slot counts");
+        const int jb32 = (int)jb, nz32 = nz, n32 = (int)n;
 #define VPD_DEFORM_CASE(C)                                                                                   \
   case C:                                                                                                    \
-    deform_pair_window<C, DAMAGE, int>(p, cnt, jb32, nz32, n32, o, h, pt, bits, live, part, fresh, near);  \
+    deform_pair_window<C, D, int>(p, cnt, jb32, nz32, n32, o, h, pt, bits, live, part, fresh, near);         \
     break;
-      switch (cnt) {
-        VPD_DEFORM_CASE(1) VPD_DEFORM_CASE(2) VPD_DEFORM_CASE(3) VPD_DEFORM_CASE(4)
-        VPD_DEFORM_CASE(5) VPD_DEFORM_CASE(6) VPD_DEFORM_CASE(7) VPD_DEFORM_CASE(8)
-        VPD_DEFORM_CASE(9) VPD_DEFORM_CASE(10) VPD_DEFORM_CASE(11) VPD_DEFORM_CASE(12)
-      default:
-        deform_pair_window<0, DAMAGE, int>(p, cnt, jb32, nz32, n32, o, h, pt, bits, live, part, fresh, near);
-      }
+        switch (cnt) {
+          VPD_DEFORM_CASE(1) VPD_DEFORM_CASE(2) VPD_DEFORM_CASE(3) VPD_DEFORM_CASE(4)
+          VPD_DEFORM_CASE(5) VPD_DEFORM_CASE(6) VPD_DEFORM_CASE(7) VPD_DEFORM_CASE(8)
+          VPD_DEFORM_CASE(9) VPD_DEFORM_CASE(10) VPD_DEFORM_CASE(11) VPD_DEFORM_CASE(12)
+        default:
+          deform_pair_window<0, D, int>(p, cnt, jb32, nz32, n32, o, h, pt, bits, live, part, fresh, near);
+        }
 #undef VPD_DEFORM_CASE
-    } else {
-      deform_pair_window<0, DAMAGE, int64_t>(p, cnt, jb, (int64_t)nz, n, o, h, pt, bits, live, part, fresh, near);
-    }
+      } else {
+        deform_pair_window<0, D, int64_t>(p, cnt, jb, (int64_t)nz, n, o, h, pt, bits, live, part, fresh, near);
+      }
+    };
+    if (tests)
+      windows(BoolConstant<DAMAGE>{});
+    else
+      windows(BoolConstant<false>{});
     if (DAMAGE)
 #pragma unroll
       for (int q = 0; q < 2; ++q)
