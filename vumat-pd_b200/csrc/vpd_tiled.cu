@@ -19,8 +19,8 @@
 // Arithmetic is that of vpd_mixed.cu: FP32 bond terms, partial sums per group (per stencil
 // plane in the packed-pair kernels) folded with Kahan compensation into the force (and in the
 // packed-pair kernels into the deformation sum),
-// the FP32 stretch test with a 1e-5 margin and the exact FP64 test inside it, pairs broken once
-// by the lower-index point.
+// the FP32 stretch test with a 1e-5 margin and the exact FP64 test inside it (in the packed
+// kernel: for every bond not clearly intact), pairs broken once by the lower-index point.
 #include "vpd_bond.cuh"
 
 namespace vpd {
@@ -52,37 +52,29 @@ __device__ __forceinline__ void stretch_test(const StepParams &p, int t, float e
   }
 }
 
-// The stretch-test decision of one bond from yy = |y|^2, xx = |xi|^2 and the tension bounds
-// thi = tension2f xx (1 + 1e-5), tlo = tension2f xx (1 - 1e-5) (stretch_test's comparisons),
-// without branches: bit t of fresh / near set where the bond at t is live (l).
-__device__ __forceinline__ void stretch_classify(const StepParams &p, int t, bool l, float yy, float xx, float thi,
-                                                 float tlo, uint32_t &fresh, uint32_t &near) {
-  bool f = yy > thi, r = !f && yy >= tlo;
-  if (p.use_compression) {  // uniform
-    const float c = p.compression2f * xx;
-    const bool cf = yy < c * (1.0f - 1.0e-5f), cr = yy <= c * (1.0f + 1.0e-5f);
-    r = r || (!f && !r && !cf && cr);
-    f = f || (!r && cf);
-  }
-  fresh |= (uint32_t)(l && f) << t;
-  near |= (uint32_t)(l && r) << t;
-}
-
 // The stretch tests of the two lanes of a packed element, paired: lane q holds a bond at window
-// position tq, tested when bit tq of live[q] is set (the arithmetic of stretch_test per lane).
+// position tq, tested when bit tq of live[q] is set. A bond whose FP32 stretch is not clearly
+// below the threshold (|y|^2 >= tension2f |xi|^2 (1 - 1e-5), or with compression not clearly
+// above its bound) sets bit tq of near[q], and the exact FP64 test (commit_breaks) decides it:
+// the same decisions as stretch_test's, whose clearly broken bonds the exact test confirms, with
+// one bit and one or two comparisons per lane.
 __device__ __forceinline__ void stretch_test2(const StepParams &p, int t0, int t1, float2 e0, float2 e1, float2 e2,
                                               float2 d0, float2 d1, float2 d2, const uint32_t (&live)[2],
-                                              uint32_t (&fresh)[2], uint32_t (&near)[2]) {
+                                              uint32_t (&near)[2]) {
   const bool l0 = (live[0] >> t0) & 1u, l1 = (live[1] >> t1) & 1u;
   if (!(l0 || l1))
     return;
   const float2 y0 = __fadd2_rn(e0, d0), y1 = __fadd2_rn(e1, d1), y2 = __fadd2_rn(e2, d2);
   const float2 yy = __ffma2_rn(y2, y2, __ffma2_rn(y1, y1, __fmul2_rn(y0, y0)));
   const float2 xx = __ffma2_rn(e2, e2, __ffma2_rn(e1, e1, __fmul2_rn(e0, e0)));
-  const float2 tt = __fmul2_rn(bcast2(p.tension2f), xx);
-  const float2 thi = __fmul2_rn(tt, bcast2(1.0f + 1.0e-5f)), tlo = __fmul2_rn(tt, bcast2(1.0f - 1.0e-5f));
-  stretch_classify(p, t0, l0, yy.x, xx.x, thi.x, tlo.x, fresh[0], near[0]);
-  stretch_classify(p, t1, l1, yy.y, xx.y, thi.y, tlo.y, fresh[1], near[1]);
+  const float2 tlo = __fmul2_rn(__fmul2_rn(bcast2(p.tension2f), xx), bcast2(1.0f - 1.0e-5f));
+  bool c0 = yy.x >= tlo.x, c1 = yy.y >= tlo.y;
+  if (p.use_compression) {  // uniform
+    const float2 chi = __fmul2_rn(__fmul2_rn(bcast2(p.compression2f), xx), bcast2(1.0f + 1.0e-5f));
+    c0 = c0 || yy.x <= chi.x, c1 = c1 || yy.y <= chi.y;
+  }
+  near[0] |= (uint32_t)(l0 && c0) << t0;
+  near[1] |= (uint32_t)(l1 && c1) << t1;
 }
 
 // ------------------------------------------------------------------ deformation
@@ -409,7 +401,7 @@ __device__ __forceinline__ void deform_pair_element(const StepParams &p, int t, 
   part[6] = __ffma2_rn(w2, e0, part[6]), part[7] = __ffma2_rn(w2, e1, part[7]);
   part[8] = __ffma2_rn(w2, e2, part[8]);
   if (DAMAGE)
-    stretch_test2(p, t, t, e0, e1, e2, d0, d1, d2, live, fresh, near);
+    stretch_test2(p, t, t, e0, e1, e2, d0, d1, d2, live, near);
 }
 
 // The two ends of a window of CNT slots as one pair: lane 0 takes position 0 (point 0's first
@@ -434,7 +426,7 @@ __device__ __forceinline__ void deform_pair_ends(const StepParams &p, I j0, I j1
   part[6] = __ffma2_rn(w2, e0, part[6]), part[7] = __ffma2_rn(w2, e1, part[7]);
   part[8] = __ffma2_rn(w2, e2, part[8]);
   if (DAMAGE)
-    stretch_test2(p, 0, CNT, e0, e1, e2, d0, d1, d2, live, fresh, near);
+    stretch_test2(p, 0, CNT, e0, e1, e2, d0, d1, d2, live, near);
 }
 
 template <int CNT, bool DAMAGE, typename I>
@@ -645,12 +637,11 @@ __global__ void __launch_bounds__(kBondThreads, 2) k_force_pair(const __grid_con
   // compensation (fc01/fc2)
   float2 fs01[2], fc01[2], part01[2];
   float fs2[2], fc2[2], part2[2];
-  double corr[2][3];
+  bool any_broken = false;  // broken bonds' corrections are rare: gathered after the sum
 #pragma unroll
   for (int q = 0; q < 2; ++q) {
     fs01[q] = fc01[q] = part01[q] = make_float2(0.0f, 0.0f);
     fs2[q] = fc2[q] = part2[q] = 0.0f;
-    corr[q][0] = corr[q][1] = corr[q][2] = 0.0;
   }
   int word = -1;  // the mask (and broken-bond) words held in mw (bw): several groups per word
   int plane = INT_MIN;
@@ -682,14 +673,7 @@ __global__ void __launch_bounds__(kBondThreads, 2) k_force_pair(const __grid_con
       uint32_t m = group_bits(mw[q], sh, cm);
       if (DAMAGE && m) {
         const uint32_t bk = m & group_bits(bw[q], sh, cm);
-        for (uint32_t f = bk; f; f &= f - 1) {  // broken bonds leave s_i
-          const int sl = pos + __ffs(f) - 1;
-          const float4 jj = p.jit[ip[q] + p.st.delta[sl]], o = p.st.e0[sl];
-          const float4 ji = p.jit[ip[q]];
-          corr[q][0] += (double)(jj.w * (o.x + (jj.x - ji.x)));
-          corr[q][1] += (double)(jj.w * (o.y + (jj.y - ji.y)));
-          corr[q][2] += (double)(jj.w * (o.z + (jj.z - ji.z)));
-        }
+        any_broken |= bk != 0u;
         m &= ~bk;
       }
       bits[q] = m << q;
@@ -727,10 +711,23 @@ __global__ void __launch_bounds__(kBondThreads, 2) k_force_pair(const __grid_con
     if (!vp[q])
       continue;
     const int64_t i = ip[q];
+    // s_i less the broken bonds' V_j xi, summed in slot order
+    double c0 = 0.0, c1 = 0.0, c2 = 0.0;
+    if (DAMAGE && any_broken) {
+      const float4 ji = p.jit[i];
+      for (int w = 0; w < p.st.nw; ++w)
+        for (uint32_t f = p.st.mask[(int64_t)w * n + i] & p.st.broken[(int64_t)w * n + i]; f; f &= f - 1) {
+          const int sl = 32 * w + __ffs(f) - 1;
+          const float4 jj = p.jit[i + p.st.delta[sl]], o = p.st.e0[sl];
+          c0 += (double)(jj.w * (o.x + (jj.x - ji.x)));
+          c1 += (double)(jj.w * (o.y + (jj.y - ji.y)));
+          c2 += (double)(jj.w * (o.z + (jj.z - ji.z)));
+        }
+    }
     float VM[9];
     fmap_rows(P0[i], P1[i], P2[i], VM);
     const double4 s = p.vxi[i];
-    const double s0 = s.x - corr[q][0], s1 = s.y - corr[q][1], s2 = s.z - corr[q][2];
+    const double s0 = s.x - c0, s1 = s.y - c1, s2 = s.z - c2;
     const double rv = 1.0 / (double)p.jit[i].w;
     const double f0 = (double)fs01[q].x + (VM[0] * s0 + VM[1] * s1 + VM[2] * s2) * rv;
     const double f1 = (double)fs01[q].y + (VM[3] * s0 + VM[4] * s1 + VM[5] * s2) * rv;
