@@ -121,23 +121,28 @@ __global__ void __launch_bounds__(kBondThreads, 2) k_deformation_tiled64(const _
       continue;
     const int64_t jb = ((int64_t)(x + gr.x) * ny + (yb * 2 + gr.z)) * nz + (z + gr.y);
     uint32_t fresh[2] = {0u, 0u};
-    if (UNROLL) {
+    // With damage, the stretch tests run (in the runtime window loop: unrolled, they spill) only
+    // for the groups where a lane of the warp has a live bond, the forward groups less their
+    // broken bonds; the other groups take the unrolled windows without tests.
+    if (DAMAGE && __any_sync(0xffffffffu, (live[0] | live[1]) != 0u)) {
+      deform64_window<0, DAMAGE, int64_t>(p, U, cnt, jb, (int64_t)nz, n, pt, ip, bits, live, G, fresh);
+    } else if (UNROLL) {
       static_assert(kUnrolledSlots == 12, "the cases below list the unrolled slot counts");
       const int jb32 = (int)jb, nz32 = nz, n32 = (int)n;
 #define VPD_DEFORM64_CASE(C)                                                                        \
   case C:                                                                                           \
-    deform64_window<C, DAMAGE, int>(p, U, cnt, jb32, nz32, n32, pt, ip, bits, live, G, fresh);      \
+    deform64_window<C, false, int>(p, U, cnt, jb32, nz32, n32, pt, ip, bits, live, G, fresh);       \
     break;
       switch (cnt) {
         VPD_DEFORM64_CASE(1) VPD_DEFORM64_CASE(2) VPD_DEFORM64_CASE(3) VPD_DEFORM64_CASE(4)
         VPD_DEFORM64_CASE(5) VPD_DEFORM64_CASE(6) VPD_DEFORM64_CASE(7) VPD_DEFORM64_CASE(8)
         VPD_DEFORM64_CASE(9) VPD_DEFORM64_CASE(10) VPD_DEFORM64_CASE(11) VPD_DEFORM64_CASE(12)
       default:
-        deform64_window<0, DAMAGE, int>(p, U, cnt, jb32, nz32, n32, pt, ip, bits, live, G, fresh);
+        deform64_window<0, false, int>(p, U, cnt, jb32, nz32, n32, pt, ip, bits, live, G, fresh);
       }
 #undef VPD_DEFORM64_CASE
     } else {
-      deform64_window<0, DAMAGE, int64_t>(p, U, cnt, jb, (int64_t)nz, n, pt, ip, bits, live, G, fresh);
+      deform64_window<0, false, int64_t>(p, U, cnt, jb, (int64_t)nz, n, pt, ip, bits, live, G, fresh);
     }
     if (DAMAGE)
 #pragma unroll
@@ -279,12 +284,14 @@ __global__ void __launch_bounds__(kBondThreads, 2) k_force_tiled64(const __grid_
 }
 
 // ------------------------------------------------------------------ launchers
-// With damage the deformation kernel keeps the runtime window loop: unrolled, the FP64 stretch
-// tests spill about 1 KB per thread and the kernel slowed from 0.96 to 1.29 ms at 1M points.
+// With damage the groups with live bonds keep the runtime window loop (unrolled, the FP64 stretch
+// tests spill about 1 KB per thread and the kernel slowed from 0.96 to 1.29 ms at 1M points); the
+// groups without take the unrolled windows without tests (0.975 to 0.90 ms from rest at 1M).
 int launch_deformation_tiled64(const StepParams &p, cudaStream_t s) {
   const unsigned grid = tiled_grid<2>(p);
   if (p.damage)
-    k_deformation_tiled64<true, false><<<grid, kBondThreads, 0, s>>>(p);
+    index32(p) ? k_deformation_tiled64<true, true><<<grid, kBondThreads, 0, s>>>(p)
+               : k_deformation_tiled64<true, false><<<grid, kBondThreads, 0, s>>>(p);
   else if (index32(p))
     k_deformation_tiled64<false, true><<<grid, kBondThreads, 0, s>>>(p);
   else
