@@ -30,6 +30,7 @@
  *                            (src/pd/CorotationalKinematics.cpp:61-149)
  *   vpd_material_update      VumatPdCorrespondenceMaterial::update (:72-176) with the
  *                            Johnson-Cook VUMAT (materials/examples/JohnsonCook.f90:12-172)
+ *   vpd_jc_return_map        the Johnson-Cook bisection alone (JohnsonCook.f90:74-136)
  *   vpd_damage_update        PdSimpleDamage::update, critical_stretch (src/damage/PdSimpleDamage.cpp:51-96);
  *                            the point modes run inside vpd_step (SimpleDamageModel.cpp:14-50)
  *   vpd_set_host_vumat       VumatMaterialAdapter (src/material/VumatMaterialAdapter.cpp:238-362)
@@ -289,6 +290,16 @@ int vpd_material_update(int64_t n, const double *props, int32_t nstatev, double 
                         double *rotation, double *strain, double *stress_corotational,
                         double *state, double *temperature, double *energy_internal,
                         double *energy_inelastic, double *stress_spatial, void *stream);
+/* The Johnson-Cook return map alone (replaces the bisection of JohnsonCook.f90:114-136, with its
+   elastic trial :74-112) on device arrays of n points: strain_inc [n x 6] (Voigt 11,22,33,23,13,12,
+   tensor shear), stress [n x 6] and state [n x nstatev] (the VUMAT's old values) -> ep_inc,
+   yield [n] and iterations [n] (0 for a point on its initialising call). method 0: the certified
+   bisection the increment kernels run (most iterations decided from two anchor evaluations of the
+   flow stress); method 1: the literal bisection, every iteration evaluated. Both give the same
+   bits. */
+int vpd_jc_return_map(int64_t n, const double *props, double dt, const double *strain_inc,
+                      const double *stress, const double *state, int32_t nstatev, int32_t method,
+                      double *ep_inc, double *yield, int32_t *iterations, void *stream);
 /* Critical-stretch bond breaking: bond_damage (per CSR entry, 0/1) updated in place,
    damage_index [n] written. */
 int vpd_damage_update(const double *positions, const double *displacement,

@@ -485,6 +485,10 @@ int create_impl(vpd_handle *h, const vpd_case *c, const double *positions, const
     const char *bk = getenv("VPD_BOND_KERNEL");
     const std::string kind = bk ? bk : "";
     p.tiled = kind == "slot" ? 0 : kind == "scalar" ? 1 : kind == "tiled2" ? 3 : kind == "staged" ? 6 : 2;
+    // VPD_RETURN_MAP=bisection: the material kernel evaluates every bisection iteration (the
+    // default decides most of them from two anchor evaluations; the results are the same)
+    const char *rm = getenv("VPD_RETURN_MAP");
+    p.literal_bisection = rm && std::string(rm) == "bisection";
   }
   if (p.st.nw && ((rc = dalloc(h, &p.vxi, n)) ||
                   (c->precision != VPD_PRECISION_MIXED && (rc = dalloc(h, &p.fmap, 3 * n)))))

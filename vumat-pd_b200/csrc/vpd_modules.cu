@@ -189,6 +189,28 @@ __global__ void k_material_update(int64_t n, JcParams jc, int nstatev, double dt
   eP[i] = pt.eInelastic;
 }
 
+// The VUMAT's return map alone for one point (JohnsonCook.f90:74-136): the elastic trial from
+// the old stress and state, then the bisection, certified (jc_return_map) or literal
+// (jc_bisection). A point on its initialising call (state[0] == 0) reports 0 iterations.
+template <bool CERTIFIED>
+__global__ void k_jc_return_map(int64_t n, JcParams jc, double dt, const double *inc, const double *sig,
+                                const double *state, int nstatev, double *epInc, double *yield, int32_t *iters) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n)
+    return;
+  JcPoint pt;
+  double d[6];
+  for (int c = 0; c < 6; ++c)
+    d[c] = inc[6 * i + c], pt.stress[c] = sig[6 * i + c], pt.state[c] = state[(size_t)nstatev * i + c];
+  pt.eInternal = pt.eInelastic = 0.0;
+  JcTrial t;
+  double e = 0.0, y = 0.0;
+  int it = 0;
+  if (jc_trial(jc, d, pt, t))
+    it = CERTIFIED ? jc_return_map(jc, dt, t, pt.state[4], e, y) : jc_bisection(jc, dt, t, pt.state[4], e, y);
+  epInc[i] = e, yield[i] = y, iters[i] = it;
+}
+
 // PdSimpleDamage::update critical_stretch (:51-82) with the reference's rounding, and the
 // damage index (:23-36).
 __global__ void k_csr_damage(const double *pos, const double *disp, const double *vol, int64_t n,
@@ -384,6 +406,25 @@ int vpd_material_update(int64_t n, const double *props, int32_t nstatev, double 
                                               temperature, energy_internal, energy_inelastic, stress_spatial, st);
   VPD_CUDA(cudaGetLastError());
   return check_status(st, s);
+}
+
+int vpd_jc_return_map(int64_t n, const double *props, double dt, const double *strain_inc, const double *stress,
+                      const double *state, int32_t nstatev, int32_t method, double *ep_inc, double *yield,
+                      int32_t *iterations, void *stream) {
+  if (!props || nstatev < 6 || !(dt > 0.0) || n < 0 || (method != 0 && method != 1))
+    return set_error(VPD_ERR_INVALID, "JC return map requires props, nstatev >= 6, dt > 0, n >= 0 and method 0 or 1.");
+  if (n == 0)
+    return VPD_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  const JcParams jc = make_jc_params(props);
+  if (method == 0)
+    k_jc_return_map<true><<<blocks(n), 128, 0, s>>>(n, jc, dt, strain_inc, stress, state, nstatev, ep_inc, yield,
+                                                   iterations);
+  else
+    k_jc_return_map<false><<<blocks(n), 128, 0, s>>>(n, jc, dt, strain_inc, stress, state, nstatev, ep_inc, yield,
+                                                    iterations);
+  VPD_CUDA(cudaGetLastError());
+  return VPD_OK;
 }
 
 int vpd_damage_update(const double *positions, const double *displacement, const double *volumes, int64_t n,

@@ -182,7 +182,9 @@ __global__ void __launch_bounds__(kBondThreads) k_deformation(StepParams p) {
 // the 250k-point bar in plastic flow than at the unconstrained 196 registers; on the 1M-point
 // bar in plastic flow 0.70 ms against 0.76 ms at three blocks per SM).
 // POINT_DAMAGE: the point damage modes (a separate instance, so the plain one keeps its registers).
-template <bool POINT_DAMAGE>
+// CERTIFIED: the return map of jc_return_map (the bisection's results with fewer flow-stress
+// evaluations); false, the literal bisection (VPD_RETURN_MAP=bisection).
+template <bool POINT_DAMAGE, bool CERTIFIED>
 __global__ void __launch_bounds__(kMaterialThreads, 4) k_material(const __grid_constant__ StepParams p) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   double part[PM_COUNT] = {};
@@ -190,7 +192,7 @@ __global__ void __launch_bounds__(kMaterialThreads, 4) k_material(const __grid_c
   if (i < p.n) {
     MaterialPoint m;
     material_load(p, i, m);
-    jc_update(p.jc, p.dt, m.inc, m.pt);
+    jc_update<CERTIFIED>(p.jc, p.dt, m.inc, m.pt);
     material_store<POINT_DAMAGE>(p, i, m, part, maxEqps);
   }
   material_reduce(p, part, maxEqps, blockIdx.x);
@@ -576,10 +578,13 @@ int launch_stage(int stage, const StepParams &p, cudaStream_t s) {
       return launch_material_host(p, s);
     if (p.surrogate)
       return launch_material_surrogate(p, s);
+    const unsigned grid = (unsigned)material_grid(p.n);
     if (p.point_damage)
-      k_material<true><<<(unsigned)material_grid(p.n), kMaterialThreads, 0, s>>>(p);
+      p.literal_bisection ? k_material<true, false><<<grid, kMaterialThreads, 0, s>>>(p)
+                          : k_material<true, true><<<grid, kMaterialThreads, 0, s>>>(p);
     else
-      k_material<false><<<(unsigned)material_grid(p.n), kMaterialThreads, 0, s>>>(p);
+      p.literal_bisection ? k_material<false, false><<<grid, kMaterialThreads, 0, s>>>(p)
+                          : k_material<false, true><<<grid, kMaterialThreads, 0, s>>>(p);
   } else if (stage == 2) {
     if (p.mixed)
       return p.tiled ? launch_force_tiled(p, s) : launch_force_mixed(p, s);

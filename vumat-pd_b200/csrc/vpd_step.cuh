@@ -69,6 +69,8 @@ struct StepParams {
   int tiled;                  // bond kernels: 0 per slot; mixed 1 tiled scalar, else packed pairs; FP64
                               // tiled with the 4-point force, 3 with the 2-point force, 6 with the
                               // TMA-staged force
+  int literal_bisection;      // 1: k_material runs the VUMAT's bisection literally (every iteration
+                              // evaluated), 0: jc_return_map (same results)
   // kinematic state
   double4 *u0, *u1;           // displacement ping-pong: increment s reads u[s & 1]
   double4 *vel, *acc, *force;

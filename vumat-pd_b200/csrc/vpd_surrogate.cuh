@@ -67,30 +67,6 @@ __device__ __forceinline__ double jc_yield0(const JcParams &p, const JcTrial &t)
   return y > t.oldYield ? y : t.oldYield;
 }
 
-// r(x) with its slope. The residual is formed exactly as in the bisection (the same flow
-// stress arithmetic, floor at oldYield, qNew clipped at 0) with one pow and one log; the slope
-// differentiates the hardening term B n ep^(n-1) = B n ep^n / ep and the rate term C / x (zero
-// at x = 0, where the VUMAT uses the reference rate).
-__device__ __forceinline__ double jc_residual(const JcParams &p, double dt, const JcTrial &t, double x,
-                                              double &slope, double &yield) {
-  const double ep = t.epOld + x, rate = x / dt;
-  const double hp = pow(ep, p.hardN), rterm = jc_rate_term(p, rate);
-  const double y = jc_flow(p, hp, t.thermal, rterm);
-  yield = y > t.oldYield ? y : t.oldYield;
-  double qNew = t.qTrial - 3.0 * p.mu * x;
-  const bool clipped = qNew <= 0.0;
-  qNew = clipped ? 0.0 : qNew;
-  double dy = 0.0;
-  if (y > t.oldYield) {
-    const double hard = p.a0 + p.b0 * hp;
-    const double dhard = ep > 0.0 ? p.b0 * p.hardN * hp / ep : 0.0;
-    const double drate = rate == 0.0 ? 0.0 : p.rateC / x;
-    dy = (dhard * rterm + hard * drate) * t.thermal;
-  }
-  slope = (clipped ? 0.0 : -3.0 * p.mu) - dy;
-  return qNew - yield;
-}
-
 // Newton on r in u = ln x from x, kept inside (0, xf] (the root's bracket). In u the rate
 // term C sigma ln(x / dt), which dominates the curvature of r at the small increments of an
 // explicit step, is linear, so the steps x <- x exp(-r / (x r'(x))) converge from guesses

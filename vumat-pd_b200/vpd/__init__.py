@@ -86,6 +86,8 @@ def library():
     lib.vpd_corotational_update.argtypes = [ctypes.c_int64, _VP, _VP, _VP, _VP, ctypes.c_double,
                                             _VP, _VP, _VP, _VP, _VP, _VP]
     lib.vpd_material_update.argtypes = [ctypes.c_int64, _D, ctypes.c_int32, ctypes.c_double] + [_VP] * 12
+    lib.vpd_jc_return_map.argtypes = [ctypes.c_int64, _D, ctypes.c_double, _VP, _VP, _VP, ctypes.c_int32,
+                                      ctypes.c_int32, _VP, _VP, _VP, _VP]
     lib.vpd_damage_update.argtypes = [_VP, _VP, _VP, ctypes.c_int64, _VP, _VP, ctypes.c_double,
                                       ctypes.c_double, _VP, _VP, _VP]
     lib.vpd_mlp_forward.argtypes = [_VP, _VP, _VP, ctypes.c_int64, _VP, _VP]
@@ -383,6 +385,22 @@ def material_update(props, dt, defgrad_new, state):
         _ptr(s["stress_corotational"]), _ptr(s["state"]), _ptr(s["temperature"]),
         _ptr(s["energy_internal"]), _ptr(s["energy_inelastic"]), _ptr(spatial), _stream()))
     return spatial
+
+
+def jc_return_map(props, dt, strain_inc, stress, state, method=0):
+    """The Johnson-Cook return map alone on CUDA tensors: strain_inc, stress [n,6], state
+    [n,nstatev] (float64) -> (ep_inc, yield, iterations) [n]. method 0: the certified bisection of
+    the increment kernels; 1: the literal bisection (the same bits)."""
+    import torch
+    n = strain_inc.shape[0]
+    props_np = np.ascontiguousarray(props, dtype=np.float64)
+    dev = strain_inc.device
+    ep = torch.empty(n, dtype=torch.float64, device=dev)
+    y = torch.empty(n, dtype=torch.float64, device=dev)
+    it = torch.empty(n, dtype=torch.int32, device=dev)
+    _check(library().vpd_jc_return_map(n, _dp(props_np), dt, _ptr(strain_inc), _ptr(stress), _ptr(state),
+                                       state.shape[1], method, _ptr(ep), _ptr(y), _ptr(it), _stream()))
+    return ep, y, it
 
 
 def mlp_forward(weight_bits, biases, x):
