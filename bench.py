@@ -14,7 +14,7 @@ step is one explicit increment of the whole bar. One process per GPU (torchrun);
 does not shard across GPUs, so N GPUs run N independent replicas ("replicas only") and the
 value is the sum of their particle-steps/s, timed as the max over ranks.
 
-Modes: plain_fp64 (FP64 bonds, the VUMAT's bisection), mixed (FP32 bond sums, the VUMAT),
+Modes: plain_fp64 (FP64 bonds, the VUMAT's bisection, certified), mixed (FP32 bond sums, the VUMAT),
 surrogate_mixed (the headline: FP32 bond sums, learned return map with the hybrid guess --
 previous plastic increment, else the network trained here by vpd_train_surrogate -- two Newton
 steps, bisection fallback), and two ablations of the guess (network only, warm start only).
