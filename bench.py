@@ -476,6 +476,12 @@ def run_gpu(args, world, rank, local):
         ws = modes["surrogate_warm_start_only_mixed"]["value"]
         gains["warm_start_only_over_mixed"] = ws / modes["mixed"]["value"]
         gains["hybrid_network_over_warm_start_only"] = head["value"] / ws
+        r = gains["hybrid_network_over_warm_start_only"]
+        gains["reading"] = (f"the gain over plain FP64 comes from the FP32 bond sums "
+                            f"({gains['mixed_over_plain_fp64']:.2f}x) and the warm-started return map "
+                            f"({gains['warm_start_only_over_mixed']:.2f}x over the mixed path's bisection); "
+                            f"the network guess {'adds' if r > 1.0 else 'costs'} {abs(r - 1.0) * 100:.0f} % "
+                            f"against the warm start alone")
     line = {
         "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
