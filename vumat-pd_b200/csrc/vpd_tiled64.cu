@@ -300,7 +300,7 @@ int launch_deformation_tiled64(const StepParams &p, cudaStream_t s) {
   return VPD_OK;
 }
 
-// four points per thread in one 512-thread block per SM (two points in 256-thread blocks with
+// three points per thread in one 384-thread block per SM (two points in 256-thread blocks with
 // VPD_BOND_KERNEL=tiled2; the TMA-staged kernel of vpd_staged64.cu with VPD_BOND_KERNEL=staged
 // where its box fits)
 int launch_force_tiled64(const StepParams &p, cudaStream_t s) {
@@ -314,15 +314,17 @@ int launch_force_tiled64(const StepParams &p, cudaStream_t s) {
       k_force_tiled64<2, false><<<grid, kBondThreads, 0, s>>>(p);
   } else {
     // A block's neighbourhood of force-map records for one stencil plane (its y-z range plus the
-    // stencil's reach, 96 bytes a point) is re-read for every group of the plane; two 256-thread
-    // blocks per SM hold two such ranges, which overflow L1. One 512-thread block per SM covers a
-    // taller y range with the same 16 warps: 0.789 against 0.821 ms at 1M points.
-    const int64_t threads = (int64_t)tiled_grid<4>(p) * kBondThreads;
-    const unsigned grid = (unsigned)((threads + 511) / 512);
+    // stencil's reach, 96 bytes a point) is re-read for every group of the plane, so it should
+    // stay in L1: three points per thread in one 384-thread block per SM (about 1150 points,
+    // a neighbourhood of about 175 KB on a 50 x 50 cross-section). On the 1M-point bar that grid
+    // is also 5.98 waves of 148 blocks. 0.616 ms at 1M points, against 0.787 for four points in
+    // 512-thread blocks (3.43 waves) and 0.821 for four points in two 256-thread blocks per SM.
+    const int64_t threads = (int64_t)tiled_grid<3>(p) * kBondThreads;
+    const unsigned grid = (unsigned)((threads + 383) / 384);
     if (index32(p))
-      k_force_tiled64<4, true, 512, 1><<<grid, 512, 0, s>>>(p);
+      k_force_tiled64<3, true, 384, 1><<<grid, 384, 0, s>>>(p);
     else
-      k_force_tiled64<4, false, 512, 1><<<grid, 512, 0, s>>>(p);
+      k_force_tiled64<3, false, 384, 1><<<grid, 384, 0, s>>>(p);
   }
   VPD_CUDA(cudaGetLastError());
   return VPD_OK;
