@@ -255,6 +255,21 @@ def test_sliced_ell_layout_matches_stencil_layout(monkeypatch):
         assert np.array_equal(b.field("damage_index"), da)
 
 
+def test_horizon_beyond_the_stencil_windows_uses_the_generic_layout():
+    """A horizon of 15 spacings on a 32-point-wide lattice makes stencil groups of 31 slots, more
+    than the tiled kernels' 32-bit windows hold for several points per thread: the case runs on
+    the sliced-ELL layout instead, and matches the oracle."""
+    case = tensile_bar(1, nx=8, ny=32, nz=4, horizon=15.015 * 0.5)
+    with vpd.Simulation(case) as sim:
+        assert sim.layout_words == 0
+        rows = sim.step(20)
+        u = sim.field("displacement")
+    o = O.OracleSim(case)
+    ref = o.step(20)
+    assert nrmse(rows[:, STRESS], ref[:, STRESS]) < 1e-9
+    assert max_rel(u, o.get("displacement")) < 1e-9
+
+
 @pytest.mark.parametrize("dims", [(24, 21, 17), (12, 37, 70)])
 @pytest.mark.parametrize("kind", ["", "staged", "staged4", "tiled2"])
 @pytest.mark.parametrize("damage", [0, 1])

@@ -143,6 +143,10 @@ int build_stencil(const int64_t *row_ptr, const int32_t *col, int64_t n, int ny,
       if (lo > hi)
         continue;
       const int count = hi - lo + 1;
+      if (count > kMaxGroupSlots) {  // a horizon above ~14 spacings: the generic layout serves it
+        cudaFree(dext), cudaFree(table);
+        return VPD_OK;
+      }
       if ((S & 31) + count > 32)
         S = (S + 31) & ~31;  // start the group in the next word
       for (int dy = lo; dy <= hi; ++dy)

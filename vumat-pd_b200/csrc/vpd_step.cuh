@@ -28,6 +28,9 @@ constexpr int kGroupBlocks = 256;   // k_integrate blocks reduced together by th
 constexpr int kBondThreads = 256;    // threads per block of the bond kernels
 constexpr int kMaterialThreads = 128;
 constexpr int kMaxStencilWords = 32; // at most 1024 lattice offsets per stencil
+// At most this many slots per stencil group: the tiled bond kernels hold a group's window for
+// their P <= 4 points per thread as bits 0 .. slots + P - 2 of one 32-bit word.
+constexpr int kMaxGroupSlots = 29;
 constexpr size_t kStagedMaxBytes = 110 * 1024;  // its box, so that two blocks fit an SM
 
 // Tiles of the TMA-staged FP64 force kernel (vpd_staged64.cu); bytes == 0: not in use.
