@@ -1,14 +1,14 @@
 // Tiled FP64 bond kernels of the plain path: the deformation gradient (with critical-stretch
-// bond breaking) and the force bond sum, two points per thread along y (the tiling of
-// vpd_tiled.cu: one load of each neighbour record per stencil-group window, consecutive
-// threads on consecutive z).
+// bond breaking), two points per thread along y, and the force bond sum, three points per
+// thread along y (the tiling of vpd_tiled.cu: one load of each neighbour record per
+// stencil-group window, consecutive threads on consecutive z).
 //
 // Each point sums its bonds in slot order with the operations of the per-slot kernels
 // (k_deformation_stencil, k_force_stencil in vpd_stencil.cu; both spell out every rounding
 // through the helpers of vpd_bond.cuh): a window position that holds no slot of the point is
 // skipped and a slot without a bond adds a zero term, as there. The results are therefore
-// bit-identical to theirs; what changes is that a neighbour's records are read once for both
-// points instead of once per point, and padding slots are not visited.
+// bit-identical to theirs; what changes is that a neighbour's records are read once for all of
+// a thread's points instead of once per point, and padding slots are not visited.
 #include "vpd_bond.cuh"
 
 namespace vpd {
